@@ -1,0 +1,215 @@
+/*
+ * zeus_b200.h -- C ABI of the B200 (sm_100a) global optimiser.
+ *
+ * Plain C: pointers, sizes, PODs; no exceptions cross it; every entry point
+ * returns ZEUS_OK (0) or a negative ZEUS_E* code, with a message available
+ * from zeus_last_error() on the calling host thread.  Device pointers are
+ * marked d_; streams are cudaStream_t passed as void* (NULL = legacy default
+ * stream).  All device entry points are asynchronous on that stream unless
+ * stated otherwise.
+ *
+ * The reference (fnal-numerics/zeus) is a header-only C++ template library
+ * with no FFI of its own; each entry point below replaces the reference
+ * function named in its comment (file:line in the reference tree), so a C,
+ * ctypes, cgo or JNI caller binds these in place of instantiating the
+ * templates.  The C++ drop-in (include/zeus.cuh, zeus::Zeus) is built on the
+ * same kernels.
+ */
+#ifndef ZEUS_B200_H
+#define ZEUS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ---------------------------------------------------- */
+#define ZEUS_OK 0
+#define ZEUS_E_INVALID (-1)     /* bad argument */
+#define ZEUS_E_UNSUPPORTED (-2) /* (objective, dim, layout) not built */
+#define ZEUS_E_CUDA (-3)        /* CUDA runtime error (launch or sync) */
+#define ZEUS_E_NOMEM (-4)       /* device allocation failed */
+#define ZEUS_E_WORKSPACE (-5)   /* workspace too small */
+
+/* ---- per-run status, the reference's Result::status (util.hpp:39-44,
+ * bfgs_common.cuh:110-273) ------------------------------------------------- */
+#define ZEUS_STATUS_UNSET (-1)
+#define ZEUS_STATUS_SURRENDER 0 /* MAX_ITER reached */
+#define ZEUS_STATUS_CONVERGED 1 /* ||grad|| < tol */
+#define ZEUS_STATUS_STOPPED 2   /* required_converged reached elsewhere */
+#define ZEUS_STATUS_NOMEM 3     /* allocation failure (whole call) */
+#define ZEUS_STATUS_KERNEL 4    /* launch / runtime failure (whole call) */
+#define ZEUS_STATUS_NONFINITE 5 /* non-finite f or ||grad|| */
+
+/* ---- built-in objectives (examples/rosenbrock.hpp, rastrigin.hpp,
+ * ackley.hpp, gaussian.hpp, simulation/fitting/LogLikelihood.h) ---------- */
+#define ZEUS_OBJ_ROSENBROCK 0
+#define ZEUS_OBJ_RASTRIGIN 1
+#define ZEUS_OBJ_ACKLEY 2
+#define ZEUS_OBJ_GAUSSIAN 3    /* 0.5 x^T C x, data = C (dim*dim) */
+#define ZEUS_OBJ_POISSON_NLL 4 /* dim 4, data = bin centres, idata = counts */
+
+#define ZEUS_PROBLEM_SYMMETRIC 1 /* zeus_problem.flags: Gaussian C = C^T */
+
+/* ---- arithmetic mode ---------------------------------------------------
+ * EXACT: the reference's operation order (O(D^3) hoisted update that equals
+ *        its O(D^4) loop, no FMA contraction, dual gradients): per-iterate
+ *        identical to the reference for polynomial objectives.
+ * FAST:  O(D^2) symmetric rank-2 update with FMA, layout by dimension,
+ *        dual or adjoint gradients.                                        */
+#define ZEUS_MODE_EXACT 0
+#define ZEUS_MODE_FAST 1
+
+#define ZEUS_GRAD_DUAL 0    /* D forward dual passes (duals.cuh:241-266) */
+#define ZEUS_GRAD_ADJOINT 1 /* hand-written reverse-mode gradient */
+
+#define ZEUS_LAYOUT_AUTO 0
+#define ZEUS_LAYOUT_THREAD 1 /* one run per thread, H in registers */
+#define ZEUS_LAYOUT_TILE 2   /* one run per 2..32-lane tile, H rows per lane */
+#define ZEUS_LAYOUT_CTA 3    /* one run per CTA, H in shared memory */
+
+typedef struct zeus_problem {
+  int32_t kind;         /* ZEUS_OBJ_* */
+  int32_t dim;          /* number of parameters D */
+  const double* data;   /* Gaussian C (row-major dim*dim) or NLL centres */
+  const int32_t* idata; /* NLL counts */
+  int32_t ndata;        /* NLL bins */
+  int32_t flags;        /* ZEUS_PROBLEM_SYMMETRIC: data matrix is symmetric */
+} zeus_problem;
+
+typedef struct zeus_bfgs_config {
+  int32_t max_iter;           /* MAX_ITER */
+  int32_t required_converged; /* stop-early threshold (> n disables) */
+  double tolerance;           /* ||grad||_2 < tolerance => converged */
+  int32_t mode;               /* ZEUS_MODE_* */
+  int32_t gradient;           /* ZEUS_GRAD_* */
+  int32_t layout;             /* ZEUS_LAYOUT_* */
+  int32_t tile;               /* lanes per run for TILE (0 = auto) */
+  int32_t block;              /* threads per block (0 = auto) */
+  int32_t reserved;
+} zeus_bfgs_config;
+
+/* Per-run outputs, all device pointers; NULL members are not written.
+ * x is row-major [run][dim].  counters (optional) receives per run
+ * {BFGS iterations, f evaluations, gradient evaluations} as int64[3].
+ * Trajectories use the reference layout [iter][dim][run] and [iter][run]
+ * (bfgs_sequential.cuh:100-109); they must hold max_iter steps and be
+ * prefilled by the caller (NaN, status -1). */
+typedef struct zeus_run_outputs {
+  double* fval;
+  int32_t* status;
+  int32_t* iter;
+  double* gnorm;
+  double* x;
+  int64_t* counters;
+  double* traj_x;
+  double* traj_f;
+  double* traj_g;
+  int8_t* traj_status;
+} zeus_run_outputs;
+
+/* The reference's Result<D> minus the coordinate array (util.hpp:36-54). */
+typedef struct zeus_result {
+  int32_t idx;
+  int32_t status;
+  double fval;
+  double gradient_norm;
+  int32_t iter;
+  int32_t reserved;
+} zeus_result;
+
+/* The reference's Convergence census (util.hpp:27-32, 151-200). */
+typedef struct zeus_census {
+  int32_t actual;      /* status 1 and within 0.5 of the known minimum */
+  int32_t claimed;     /* status 1 */
+  int32_t surrendered; /* any status other than 1 and 2 */
+  int32_t stopped;     /* status 2 */
+  int32_t best_idx;    /* argmin fval (lowest index on ties) */
+  int32_t reserved;
+} zeus_census;
+
+/* ---- runtime -------------------------------------------------------- */
+/* Message of the last failing call on this host thread ("" if none). */
+const char* zeus_last_error(void);
+/* Library version string. */
+const char* zeus_version(void);
+/* 1 if (problem kind, dim) has built kernels for (mode, gradient). */
+int zeus_supported(int32_t kind, int32_t dim, int32_t mode, int32_t gradient);
+
+/* ---- starts ---------------------------------------------------------
+ * Uniform starts in [lower, upper) from Philox4x32-10, counter = run index:
+ * d_out[i*dim+d].  Replaces the reference's in-kernel cuRAND draws when
+ * PSO is off (bfgs_sequential.cuh:73-77, utils.cuh:353-358). */
+int zeus_starts_uniform(uint64_t seed, int64_t n, int32_t dim, double lower,
+                        double upper, double* d_out, void* stream);
+
+/* ---- PSO seeding ----------------------------------------------------
+ * Replaces pso::launch (pso.cuh:194-345; kernels 17-155): init plus `iters`
+ * synchronous PSO steps (gBest fixed at each iteration boundary by a
+ * deterministic argmin, ties to the lowest index), all launched on `stream`
+ * with no host round trip.  Outputs the per-particle best positions (the
+ * BFGS starts, d_pbest_x[n*dim]) and values; d_gbest receives {f, x[dim]}.
+ * Workspace: zeus_pso_workspace_size() bytes of device memory. */
+size_t zeus_pso_workspace_size(int64_t n, int32_t dim);
+int zeus_pso_device(const zeus_problem* problem, uint64_t seed, int64_t n,
+                    double lower, double upper, int32_t iters, double w,
+                    double c1, double c2, double* d_pbest_x,
+                    double* d_pbest_f, double* d_gbest, void* d_workspace,
+                    size_t workspace_bytes, void* stream);
+
+/* ---- BFGS -----------------------------------------------------------
+ * Replaces bfgs::sequential::launch / bfgs::parallel::launch
+ * (bfgs_sequential.cuh:384-589, bfgs_parallel.cuh:301-472) and their
+ * kernels: one FP64 BFGS per start d_starts[i*dim+d], with the reference's
+ * line search, update skip, accept-if-better and termination protocol.
+ * d_control: 2 int32 {stop flag, converged count}, zeroed by the caller
+ * before the first launch (the reference's BFGSContext, context.hpp:7-10).
+ * Workspace: zeus_bfgs_workspace_size() bytes (0 for most layouts). */
+size_t zeus_bfgs_workspace_size(const zeus_problem* problem,
+                                const zeus_bfgs_config* config, int64_t n);
+int zeus_bfgs_device(const zeus_problem* problem,
+                     const zeus_bfgs_config* config, const double* d_starts,
+                     int64_t n, const zeus_run_outputs* out,
+                     int32_t* d_control, void* d_workspace,
+                     size_t workspace_bytes, void* stream);
+
+/* ---- reduction ------------------------------------------------------
+ * Replaces bfgs::launchReduction + util::dumpDataToFile's census
+ * (bfgs_common.cuh:280-319, util.hpp:151-200): argmin of fval (lowest index
+ * on ties, NaN never wins) and status counts, in one kernel.  known_min is a
+ * HOST pointer to dim doubles (NULL: origin) used for `actual`. */
+int zeus_census_device(const double* d_fval, const int32_t* d_status,
+                       const double* d_x, int64_t n, int32_t dim,
+                       const double* known_min, zeus_census* d_census,
+                       void* stream);
+
+/* ---- whole call with host buffers -------------------------------------
+ * The drop-in for zeus::Zeus (zeus.cuh:341-375) on a built-in objective:
+ * problem data in HOST memory, PSO (pso_iter >= 0; pso_iter < 0 draws
+ * uniform starts), BFGS, argmin and census; synchronous.  Copies the best
+ * run into *best / best_x (host, dim doubles) and, when per_run_* are not
+ * NULL, every run's fval/status (host arrays of n).  Returns ZEUS_OK, or an
+ * error code with best->status set to 3 (allocation) or 4 (CUDA), as the
+ * reference does (zeus.cuh:112-116). */
+int zeus_optimize(const zeus_problem* host_problem, double lower,
+                  double upper, int64_t n, int32_t max_iter, int32_t pso_iter,
+                  int32_t required_converged, double tolerance, uint64_t seed,
+                  const zeus_bfgs_config* config, zeus_result* best,
+                  double* best_x, zeus_census* census, double* per_run_fval,
+                  int32_t* per_run_status, void* stream);
+
+/* ---- measurement ----------------------------------------------------
+ * No counterpart in the reference: a roofline probe.  Runs `iters`
+ * iterations of 8 independent FP64 FMA chains per thread on a grid sized to
+ * fill every SM, and writes one double per thread to d_sink (grid*block
+ * doubles, see zeus_probe_fp64_shape) so the work cannot be elided.  Flops =
+ * grid * block * iters * 8 * 2; time it with events on `stream`. */
+void zeus_probe_fp64_shape(int32_t* grid, int32_t* block);
+int zeus_probe_fp64(int64_t iters, double* d_sink, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

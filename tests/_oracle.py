@@ -1,0 +1,171 @@
+"""ctypes access to the checkers: the C restatement (oracle/libzeus_oracle.so)
+and the reference's own sequential BFGS compiled for the host
+(oracle/_ref/libzeus_ref.so).  Test infrastructure only."""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent.parent
+ORACLE_SO = ROOT / "oracle" / "libzeus_oracle.so"
+REF_SO = ROOT / "oracle" / "_ref" / "libzeus_ref.so"
+
+_P = C.c_void_p
+_BFGS_SIG = [C.c_int, C.c_int, _P, _P, C.c_int, _P, C.c_int, C.c_double, C.c_double,
+             C.c_int, C.c_int, C.c_double, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_int]
+
+
+class ZorObjective(C.Structure):
+    _fields_ = [("kind", C.c_int), ("dim", C.c_int), ("data", _P), ("idata", _P),
+                ("ndata", C.c_int)]
+
+
+_oracle = None
+_ref = None
+
+
+def oracle():
+    global _oracle
+    if _oracle is None:
+        L = C.CDLL(str(ORACLE_SO))
+        L.zor_bfgs.argtypes = _BFGS_SIG
+        L.zor_value.restype = C.c_double
+        L.zor_value.argtypes = [C.POINTER(ZorObjective), _P]
+        L.zor_value_grad_dual.restype = C.c_double
+        L.zor_value_grad_dual.argtypes = [C.POINTER(ZorObjective), _P, _P]
+        L.zor_value_grad_analytic.restype = C.c_double
+        L.zor_value_grad_analytic.argtypes = [C.POINTER(ZorObjective), _P, _P]
+        L.zor_digamma.restype = C.c_double
+        L.zor_digamma.argtypes = [C.c_double]
+        L.zor_line_search.restype = C.c_double
+        L.zor_line_search.argtypes = [C.POINTER(ZorObjective), C.c_double, _P, _P, _P]
+        L.zor_bfgs_update.argtypes = [C.c_int, _P, _P, _P, C.c_double]
+        L.zor_uniform.restype = C.c_double
+        L.zor_uniform.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32]
+        L.zor_uniform_starts.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_double,
+                                         C.c_double, _P]
+        L.zor_philox4x32_10.argtypes = [_P, _P, _P]
+        L.zor_pso.argtypes = [C.POINTER(ZorObjective), C.c_uint64, C.c_int, C.c_double,
+                              C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
+                              _P, _P, _P, _P]
+        L.zor_pso_step.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _P, _P,
+                                   _P, _P, _P, _P]
+        _oracle = L
+    return _oracle
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        L = C.CDLL(str(REF_SO))
+        L.zref_bfgs.argtypes = _BFGS_SIG
+        L.zref_linesearch_quadratic.restype = C.c_double
+        L.zref_linesearch_quadratic.argtypes = [C.c_double] * 4
+        L.zref_bfgs_update.argtypes = [C.c_int, _P, _P, _P, C.c_double]
+        L.zref_digamma.restype = C.c_double
+        L.zref_digamma.argtypes = [C.c_double]
+        L.zref_value_grad.restype = C.c_double
+        L.zref_value_grad.argtypes = [C.c_int, C.c_int, _P, _P]
+        _ref = L
+    return _ref
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def zobj(kind, dim, data=None, idata=None):
+    nd = 0 if idata is None else len(idata)
+    return ZorObjective(kind, dim, _p(data), _p(idata), nd)
+
+
+def run_bfgs(fn, kind, dim, starts, max_iter=1000, required=None, tol=1e-8,
+             data=None, idata=None, traj=False, lower=-5.0, upper=5.0, nthreads=1):
+    """Calls zor_bfgs / zref_bfgs; returns dict of numpy arrays."""
+    starts = np.ascontiguousarray(starts, dtype=np.float64)
+    n = starts.shape[0]
+    if required is None:
+        required = n + 1
+    out = dict(fval=np.zeros(n), status=np.zeros(n, np.int32), iter=np.zeros(n, np.int32),
+               gnorm=np.zeros(n), x=np.zeros((n, dim)))
+    tx = tf = tg = ts = None
+    if traj:
+        tx = np.full((max_iter, dim, n), np.nan)
+        tf = np.full((max_iter, n), np.nan)
+        tg = np.full((max_iter, n), np.nan)
+        ts = np.full((max_iter, n), -1, np.int8)
+    nd = 0 if idata is None else len(idata)
+    rc = fn(kind, dim, _p(data), _p(idata), nd, _p(starts), n, lower, upper, max_iter,
+            required, tol, _p(out["fval"]), _p(out["status"]), _p(out["iter"]),
+            _p(out["gnorm"]), _p(out["x"]), _p(tx), _p(tf), _p(tg), _p(ts), nthreads)
+    assert rc == 0, f"bfgs returned {rc}"
+    if traj:
+        out.update(traj_x=tx, traj_f=tf, traj_g=tg, traj_status=ts)
+    return out
+
+
+def oracle_bfgs(*a, **k):
+    return run_bfgs(oracle().zor_bfgs, *a, **k)
+
+
+def ref_bfgs(*a, **k):
+    return run_bfgs(ref().zref_bfgs, *a, **k)
+
+
+def oracle_starts(seed, n, dim, lower, upper):
+    out = np.zeros((n, dim))
+    oracle().zor_uniform_starts(seed, n, dim, lower, upper, _p(out))
+    return out
+
+
+def oracle_pso(kind, dim, seed, n, lower, upper, iters, w=0.5, c1=1.2, c2=1.5,
+               data=None, idata=None):
+    o = zobj(kind, dim, data, idata)
+    pbx = np.zeros((n, dim))
+    pbf = np.zeros(n)
+    gbx = np.zeros(dim)
+    gbf = np.zeros(1)
+    oracle().zor_pso(C.byref(o), seed, n, lower, upper, iters, w, c1, c2, _p(pbx),
+                     _p(pbf), _p(gbx), _p(gbf))
+    return pbx, pbf, gbx, gbf[0]
+
+
+def value(kind, dim, x, data=None, idata=None):
+    o = zobj(kind, dim, data, idata)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    return oracle().zor_value(C.byref(o), _p(x))
+
+
+def grad_dual(kind, dim, x, data=None, idata=None):
+    o = zobj(kind, dim, data, idata)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    g = np.zeros(dim)
+    f = oracle().zor_value_grad_dual(C.byref(o), _p(x), _p(g))
+    return f, g
+
+
+def grad_analytic(kind, dim, x, data=None, idata=None):
+    o = zobj(kind, dim, data, idata)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    g = np.zeros(dim)
+    f = oracle().zor_value_grad_analytic(C.byref(o), _p(x), _p(g))
+    return f, g
+
+
+def dijet_toy(seed=7, nbins=100, total=1e6, p=(1e6, 10.0, 5.0, 0.1)):
+    """Synthetic binned dijet spectrum: 100 log-spaced bins in x = m/13000
+    over [0.085, 0.54], lambda_i = p0 (1-x)^p1 / x^(p2 + p3 ln x) at bin
+    centres rescaled to `total` events, counts ~ Poisson(lambda)."""
+    edges = np.geomspace(0.085, 0.54, nbins + 1)
+    x = 0.5 * (edges[1:] + edges[:-1])
+    lam = p[0] * (1 - x) ** p[1] / x ** (p[2] + p[3] * np.log(x))
+    lam *= total / lam.sum()
+    rng = np.random.default_rng(seed)
+    k = rng.poisson(lam).astype(np.int32)
+    return x, k, lam

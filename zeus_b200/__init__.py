@@ -1,0 +1,332 @@
+"""zeus_b200: B200 (sm_100a) FP64 global optimiser behind the zeus::Zeus API.
+
+Host-side Python mirror of the reference's entry point
+``zeus::Zeus(f, lower, upper, N, MAX_ITER, PSO_ITER, requiredConverged,
+fun_name, tolerance, seed, run, parallel, prng, trajectory_file, nzerosteps)``
+(include/zeus.cuh:341-375 in the reference), bound to the C ABI in
+include/zeus_b200.h through ctypes.  The compute path is the CUDA library
+``libzeus_b200.so`` built in-tree by ``zeus_b200/build.py``; there is no CPU
+fallback: if the library is missing or a call fails, an exception is raised.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import os
+from pathlib import Path
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libzeus_b200.so"
+
+# ---- constants mirrored from include/zeus_b200.h -------------------------
+OK = 0
+E_INVALID, E_UNSUPPORTED, E_CUDA, E_NOMEM, E_WORKSPACE = -1, -2, -3, -4, -5
+STATUS_SURRENDER, STATUS_CONVERGED, STATUS_STOPPED = 0, 1, 2
+STATUS_NOMEM, STATUS_KERNEL, STATUS_NONFINITE = 3, 4, 5
+OBJ_ROSENBROCK, OBJ_RASTRIGIN, OBJ_ACKLEY, OBJ_GAUSSIAN, OBJ_POISSON_NLL = range(5)
+PROBLEM_SYMMETRIC = 1
+MODE_EXACT, MODE_FAST = 0, 1
+GRAD_DUAL, GRAD_ADJOINT = 0, 1
+LAYOUT_AUTO, LAYOUT_THREAD, LAYOUT_TILE, LAYOUT_CTA = 0, 1, 2, 3
+
+_MODES = {"exact": MODE_EXACT, "fast": MODE_FAST}
+_GRADS = {"dual": GRAD_DUAL, "adjoint": GRAD_ADJOINT}
+
+
+class ZeusError(RuntimeError):
+    """A C-ABI call returned an error code."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"zeus_b200 error {code}: {msg}")
+        self.code = code
+
+
+class Problem(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("dim", C.c_int32),
+        ("data", C.c_void_p),
+        ("idata", C.c_void_p),
+        ("ndata", C.c_int32),
+        ("flags", C.c_int32),
+    ]
+
+
+class BfgsConfig(C.Structure):
+    _fields_ = [
+        ("max_iter", C.c_int32),
+        ("required_converged", C.c_int32),
+        ("tolerance", C.c_double),
+        ("mode", C.c_int32),
+        ("gradient", C.c_int32),
+        ("layout", C.c_int32),
+        ("tile", C.c_int32),
+        ("block", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class RunOutputs(C.Structure):
+    _fields_ = [
+        ("fval", C.c_void_p),
+        ("status", C.c_void_p),
+        ("iter", C.c_void_p),
+        ("gnorm", C.c_void_p),
+        ("x", C.c_void_p),
+        ("counters", C.c_void_p),
+        ("traj_x", C.c_void_p),
+        ("traj_f", C.c_void_p),
+        ("traj_g", C.c_void_p),
+        ("traj_status", C.c_void_p),
+    ]
+
+
+class CResult(C.Structure):
+    _fields_ = [
+        ("idx", C.c_int32),
+        ("status", C.c_int32),
+        ("fval", C.c_double),
+        ("gradient_norm", C.c_double),
+        ("iter", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class CCensus(C.Structure):
+    _fields_ = [
+        ("actual", C.c_int32),
+        ("claimed", C.c_int32),
+        ("surrendered", C.c_int32),
+        ("stopped", C.c_int32),
+        ("best_idx", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+# Every symbol include/zeus_b200.h declares: (name, restype, argtypes).
+_P = C.c_void_p
+SIGNATURES = {
+    "zeus_last_error": (C.c_char_p, []),
+    "zeus_version": (C.c_char_p, []),
+    "zeus_supported": (C.c_int, [C.c_int32] * 4),
+    "zeus_starts_uniform": (
+        C.c_int,
+        [C.c_uint64, C.c_int64, C.c_int32, C.c_double, C.c_double, _P, _P],
+    ),
+    "zeus_pso_workspace_size": (C.c_size_t, [C.c_int64, C.c_int32]),
+    "zeus_pso_device": (
+        C.c_int,
+        [C.POINTER(Problem), C.c_uint64, C.c_int64, C.c_double, C.c_double,
+         C.c_int32, C.c_double, C.c_double, C.c_double, _P, _P, _P, _P,
+         C.c_size_t, _P],
+    ),
+    "zeus_bfgs_workspace_size": (
+        C.c_size_t, [C.POINTER(Problem), C.POINTER(BfgsConfig), C.c_int64]),
+    "zeus_bfgs_device": (
+        C.c_int,
+        [C.POINTER(Problem), C.POINTER(BfgsConfig), _P, C.c_int64,
+         C.POINTER(RunOutputs), _P, _P, C.c_size_t, _P],
+    ),
+    "zeus_census_device": (
+        C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, _P, _P, _P]),
+    "zeus_optimize": (
+        C.c_int,
+        [C.POINTER(Problem), C.c_double, C.c_double, C.c_int64, C.c_int32,
+         C.c_int32, C.c_int32, C.c_double, C.c_uint64, C.POINTER(BfgsConfig),
+         C.POINTER(CResult), _P, C.POINTER(CCensus), _P, _P, _P],
+    ),
+    "zeus_probe_fp64_shape": (None, [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "zeus_probe_fp64": (C.c_int, [C.c_int64, _P, _P]),
+}
+
+_lib: Optional[C.CDLL] = None
+
+
+def lib() -> C.CDLL:
+    """The loaded CUDA library; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python zeus_b200/build.py` "
+                "(the CUDA library is the only compute path)")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().zeus_last_error().decode()
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        raise ZeusError(rc, last_error())
+
+
+def supported(kind: int, dim: int, mode: str = "fast", gradient: str = "adjoint") -> bool:
+    return bool(lib().zeus_supported(kind, dim, _MODES[mode], _GRADS[gradient]))
+
+
+# ---- objectives ------------------------------------------------------------
+@dataclasses.dataclass
+class Objective:
+    """A built-in objective: kind, dimension and host-side data."""
+
+    kind: int
+    dim: int
+    data: Optional[np.ndarray] = None   # Gaussian C / NLL bin centres
+    idata: Optional[np.ndarray] = None  # NLL counts
+    name: str = ""
+
+    def problem(self, data_ptr=None, idata_ptr=None, flags=None) -> Problem:
+        """C struct with the given (device or host) data pointers."""
+        nd = 0 if self.idata is None else len(self.idata)
+        if flags is None:
+            flags = 0
+            if self.kind == OBJ_GAUSSIAN and self.data is not None and np.array_equal(
+                    self.data, self.data.T):
+                flags = PROBLEM_SYMMETRIC
+        return Problem(self.kind, self.dim, data_ptr, idata_ptr, nd, flags)
+
+    def host_problem(self) -> Problem:
+        d = None if self.data is None else self.data.ctypes.data
+        i = None if self.idata is None else self.idata.ctypes.data
+        return self.problem(d, i)
+
+    @property
+    def known_minimum(self) -> Optional[np.ndarray]:
+        if self.kind == OBJ_ROSENBROCK:
+            return np.ones(self.dim)
+        return None
+
+
+def Rosenbrock(dim: int) -> Objective:
+    """examples/rosenbrock.hpp: sum (1-x_i)^2 + 100 (x_{i+1}-x_i^2)^2."""
+    return Objective(OBJ_ROSENBROCK, dim, name="rosenbrock")
+
+
+def Rastrigin(dim: int) -> Objective:
+    """examples/rastrigin.hpp: 10 D + sum x_i^2 - 10 cos(2 pi x_i)."""
+    return Objective(OBJ_RASTRIGIN, dim, name="rastrigin")
+
+
+def Ackley(dim: int) -> Objective:
+    """examples/ackley.hpp (a=20, b=0.2, c=2 pi)."""
+    return Objective(OBJ_ACKLEY, dim, name="ackley")
+
+
+def Gaussian(C_matrix) -> Objective:
+    """examples/gaussian.hpp: 0.5 x^T C x with dense C (D x D)."""
+    Cm = np.ascontiguousarray(np.asarray(C_matrix, dtype=np.float64))
+    if Cm.ndim != 2 or Cm.shape[0] != Cm.shape[1]:
+        raise ValueError("C must be square")
+    return Objective(OBJ_GAUSSIAN, Cm.shape[0], data=Cm, name="gaussian")
+
+
+def PoissonNLL(counts, centres) -> Objective:
+    """simulation/fitting/LogLikelihood.h: binned Poisson NLL, 4 parameters."""
+    k = np.ascontiguousarray(np.asarray(counts, dtype=np.int32))
+    x = np.ascontiguousarray(np.asarray(centres, dtype=np.float64))
+    if k.shape != x.shape or k.ndim != 1 or len(k) == 0:
+        raise ValueError("counts and centres must be equal-length 1-D arrays")
+    return Objective(OBJ_POISSON_NLL, 4, data=x, idata=k, name="poisson")
+
+
+def gaussian_matrix(dim: int, off: float = 0.5) -> np.ndarray:
+    """C_ii = 1 + (dim-1) off, C_ij = off: the reference's Gaussian example
+    (C_ii = 1 + 149 * 0.5 = 75.5 at dim 150)."""
+    C_m = np.full((dim, dim), off)
+    np.fill_diagonal(C_m, 1.0 + (dim - 1) * off)
+    return C_m
+
+
+# ---- the reference's result types -----------------------------------------
+@dataclasses.dataclass
+class Convergence:
+    """util.hpp:27-32."""
+
+    actual: int = 0
+    claimed: int = 0
+    surrendered: int = 0
+    stopped: int = 0
+
+
+@dataclasses.dataclass
+class Result:
+    """zeus::Result<D> (util.hpp:36-54)."""
+
+    idx: int = -1
+    status: int = -1
+    fval: float = 37.0
+    gradientNorm: float = 0.0
+    coordinates: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(0))
+    iter: int = 0
+    c: Convergence = dataclasses.field(default_factory=Convergence)
+    per_run_fval: Optional[np.ndarray] = None
+    per_run_status: Optional[np.ndarray] = None
+
+
+def make_config(max_iter: int, required: int, tol: float, mode: str = "fast",
+                gradient: str = "adjoint", layout: int = LAYOUT_AUTO, tile: int = 0,
+                block: int = 0) -> BfgsConfig:
+    return BfgsConfig(max_iter, required, tol, _MODES[mode], _GRADS[gradient],
+                      layout, tile, block, 0)
+
+
+def Zeus(f: Objective, lower: float, upper: float, N: int, MAX_ITER: int,
+         PSO_ITER: int, requiredConverged: int, fun_name: str = "",
+         tolerance: float = 1e-8, seed: int = 42, run: int = 0,
+         parallel: bool = True, prng=None, trajectory_file: str = "",
+         nzerosteps: int = 0, *, mode: str = "fast", gradient: str = "adjoint",
+         per_run: bool = False, stream=None) -> Result:
+    """The reference's zeus::Zeus on a built-in objective, host buffers in and
+    out.  ``parallel``/``prng``/``trajectory_file``/``nzerosteps`` are accepted
+    for signature compatibility: the layout is chosen by dimension, the
+    generator is Philox, per-iteration trajectories come from exact mode
+    through bfgs_device(), and the zero-step limit cannot trigger because the
+    reference's line search never returns 0 (utils.cuh:395-411)."""
+    del parallel, prng, run, nzerosteps, fun_name
+    if trajectory_file:
+        raise NotImplementedError("trajectory files: use bfgs_device(..., traj=True)")
+    if N < 0:
+        raise ValueError("N must be >= 0")
+    cfg = make_config(MAX_ITER, requiredConverged, tolerance, mode, gradient)
+    best = CResult()
+    census = CCensus()
+    bx = np.zeros(f.dim)
+    pf = np.zeros(max(N, 1)) if per_run else None
+    ps = np.zeros(max(N, 1), dtype=np.int32) if per_run else None
+    rc = lib().zeus_optimize(
+        C.byref(f.host_problem()), lower, upper, N, MAX_ITER, PSO_ITER,
+        requiredConverged, tolerance, seed & 0xFFFFFFFFFFFFFFFF, C.byref(cfg),
+        C.byref(best), bx.ctypes.data, C.byref(census),
+        None if pf is None else pf.ctypes.data,
+        None if ps is None else ps.ctypes.data, stream)
+    r = Result(idx=best.idx, status=best.status, fval=best.fval,
+               gradientNorm=best.gradient_norm, coordinates=bx, iter=best.iter,
+               c=Convergence(census.actual, census.claimed, census.surrendered,
+                             census.stopped))
+    if per_run and N > 0:
+        r.per_run_fval, r.per_run_status = pf[:N], ps[:N]
+    if rc != OK:
+        if rc in (E_NOMEM, E_CUDA):
+            return r  # status 3 / 4 as the reference reports them
+        check(rc)
+    return r
+
+
+from .device import bfgs_device, pso_device, starts_uniform, census_device  # noqa: E402
+
+__all__ = [
+    "Zeus", "Result", "Convergence", "Objective", "Rosenbrock", "Rastrigin",
+    "Ackley", "Gaussian", "PoissonNLL", "gaussian_matrix", "bfgs_device",
+    "pso_device", "starts_uniform", "census_device", "lib", "supported",
+]

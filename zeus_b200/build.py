@@ -1,0 +1,89 @@
+"""Builds zeus_b200/libzeus_b200.so (sm_100a) in-tree with nvcc.
+
+Each translation unit compiles in parallel; an object is rebuilt only when
+it is older than any source or header under csrc/ or include/.  The
+exact-mode unit is compiled with -fmad=false (no multiply-add contraction).
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent
+CSRC = HERE / "csrc"
+INCLUDE = ROOT / "include"
+BUILD = HERE / "_build"
+LIB = HERE / "libzeus_b200.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = [
+    "-std=c++20",
+    "--expt-relaxed-constexpr",
+    "-O3",
+    "-lineinfo",
+    "-Xcompiler",
+    "-fPIC",
+    "-I",
+    str(INCLUDE),
+    "-I",
+    str(CSRC),
+] + ARCH
+
+# (source, extra flags)
+UNITS = [
+    ("zb_exact.cu", ["-fmad=false"]),
+    ("zb_fast.cu", []),
+    ("zb_runtime.cu", []),
+]
+
+
+def nvcc() -> str:
+    exe = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(exe).exists():
+        raise RuntimeError("nvcc not found: the CUDA toolkit is required to build")
+    return exe
+
+
+def _deps_mtime() -> float:
+    files = list(CSRC.glob("*")) + list(INCLUDE.glob("*.h")) + [Path(__file__)]
+    return max(f.stat().st_mtime for f in files if f.is_file())
+
+
+def _compile(src: str, extra: list[str], newest: float, verbose: bool) -> Path:
+    obj = BUILD / (Path(src).stem + ".o")
+    if obj.exists() and obj.stat().st_mtime >= newest:
+        return obj
+    cmd = [nvcc(), *COMMON, *extra, "-c", str(CSRC / src), "-o", str(obj)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+    return obj
+
+
+def build(verbose: bool = False, jobs: int | None = None) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    newest = _deps_mtime()
+    with cf.ThreadPoolExecutor(max_workers=jobs or len(UNITS)) as ex:
+        objs = list(ex.map(lambda u: _compile(u[0], u[1], newest, verbose), UNITS))
+    if LIB.exists() and LIB.stat().st_mtime >= max(o.stat().st_mtime for o in objs):
+        return LIB
+    tmp = LIB.with_suffix(".so.tmp")
+    cmd = [nvcc(), "-shared", *ARCH, "-o", str(tmp), *map(str, objs)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

@@ -1,0 +1,97 @@
+// Shared device-side types and helpers for the BFGS / PSO kernels.
+#pragma once
+
+#include <array>
+#include <concepts>
+#include <cstddef>
+#include <cstdint>
+#include <type_traits>
+
+#include "zb_dual.cuh"
+
+namespace zb {
+
+  // Status codes of the reference's Result::status (util.hpp:39-44).
+  enum : int {
+    kUnset = -1,
+    kSurrender = 0,
+    kConverged = 1,
+    kStopped = 2,
+    kNonFinite = 5
+  };
+
+  // Line-search constants (utils.cuh:389-395) and the update skip threshold
+  // (utils.cuh:254-255).
+  inline constexpr double kArmijoC1 = 0.1;
+  inline constexpr int kLineSearchTrials = 20;
+  inline constexpr double kMinCurvature = 1e-14;
+
+  struct BfgsParams {
+    int64_t n;
+    int max_iter;
+    int required;
+    double tol;
+  };
+
+  // Device view of zeus_run_outputs (include/zeus_b200.h).
+  struct RunOut {
+    double* fval;
+    int32_t* status;
+    int32_t* iter;
+    double* gnorm;
+    double* x;
+    int64_t* counters; // [run][3]: iterations, f evaluations, gradients
+    double* traj_x;
+    double* traj_f;
+    double* traj_g;
+    int8_t* traj_status;
+  };
+
+  // {stop flag, converged count}: the reference's BFGSContext
+  // (context.hpp:7-10), device-global.
+  struct Control {
+    int stop;
+    int converged;
+  };
+
+  template <class F>
+  concept HasValue = requires(const F& f, const double* x) {
+    { f.value(x) } -> std::convertible_to<double>;
+  };
+  template <class F>
+  concept HasAdjoint = requires(const F& f, const double* x, double* g) {
+    { f.adjoint(x, g) } -> std::convertible_to<double>;
+  };
+
+  // Relaxed read of the stop flag, issued once per BFGS iteration like the
+  // reference's atomicAdd(&stopFlag, 0) (bfgs_common.cuh:127).
+  __device__ __forceinline__ int
+  load_stop(const Control* c)
+  {
+    return *reinterpret_cast<const volatile int*>(&c->stop);
+  }
+
+  // Marks one more converged run; raises the stop flag at `required`
+  // (bfgs_common.cuh:184-193).
+  __device__ __forceinline__ void
+  note_converged(Control* c, int required)
+  {
+    const int old = atomicAdd(&c->converged, 1);
+    if (old + 1 == required) {
+      atomicExch(&c->stop, 1);
+      __threadfence();
+    }
+  }
+
+  // fval as an unsigned key ordered like the doubles; NaN maps above +inf so
+  // it never wins a min.
+  __device__ __forceinline__ unsigned long long
+  order_key(double f)
+  {
+    if (f != f)
+      return ~0ull;
+    unsigned long long b = (unsigned long long)__double_as_longlong(f);
+    return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+  }
+
+} // namespace zb

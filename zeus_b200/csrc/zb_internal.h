@@ -1,0 +1,61 @@
+// Host-side interface between the library's translation units:
+//   zb_exact.cu  (-fmad=false): exact-mode BFGS and PSO launchers
+//   zb_fast.cu   : fast-mode BFGS launchers (thread / tile / CTA layouts)
+//   zb_runtime.cu: the C ABI (include/zeus_b200.h), reductions, orchestration
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "zeus_b200.h"
+#include "zb_common.cuh"
+
+namespace zb {
+
+  // A built-in objective with its data resolved to device pointers.
+  struct Objective {
+    int kind;
+    int dim;
+    const double* data;    // Gaussian C / NLL centres
+    const int* idata;      // NLL counts
+    int ndata;             // NLL bins
+    int flags;             // bit 0: Gaussian C is symmetric
+    const double* nll_bins; // NLL {ln x, ln(1-x), k, lgamma(k+1)} per bin
+  };
+
+  void set_error(const char* fmt, ...);
+  int cuda_fail(cudaError_t e, const char* what);
+  int sm_count();
+
+  // exact mode (zb_exact.cu)
+  bool exact_supported(int kind, int dim);
+  size_t exact_workspace_bytes(const Objective& o, int64_t n);
+  int launch_exact(const Objective& o, const BfgsParams& prm,
+                   const double* starts, const RunOut& out, Control* ctl,
+                   void* ws, size_t ws_bytes, cudaStream_t st);
+
+  // PSO (zb_exact.cu)
+  bool pso_supported(int kind, int dim);
+  size_t pso_workspace_bytes(int64_t n, int dim);
+  int launch_pso(const Objective& o, uint64_t seed, int64_t n, double lower,
+                 double upper, int iters, double w, double c1, double c2,
+                 double* pbx, double* pbf, double* gbest, void* ws,
+                 size_t ws_bytes, cudaStream_t st);
+
+  // fast mode (zb_fast.cu)
+  bool fast_supported(int kind, int dim, int gradient);
+  size_t fast_workspace_bytes(const Objective& o, const zeus_bfgs_config& c,
+                              int64_t n);
+  int launch_fast(const Objective& o, const zeus_bfgs_config& c,
+                  const BfgsParams& prm, const double* starts,
+                  const RunOut& out, Control* ctl, void* ws, size_t ws_bytes,
+                  cudaStream_t st);
+
+  inline size_t
+  align_up(size_t v, size_t a = 256)
+  {
+    return (v + a - 1) / a * a;
+  }
+
+} // namespace zb

@@ -1,0 +1,334 @@
+// Built-in objectives: the reference's benchmark functions
+// (examples/rosenbrock.hpp:6-41, rastrigin.hpp:6-38, ackley.hpp:10-50,
+// gaussian.hpp:8-34, simulation/fitting/LogLikelihood.h:12-82).
+//
+// Each objective has three entry points:
+//  * operator()(std::array<T, D>) for T = double and dual::DualNumber, with
+//    the reference's expression order (the `if constexpr` branches exist
+//    because the reference writes its double and dual bodies differently);
+//    exact mode and dual gradients use only this;
+//  * value(x): the same function in FMA-friendly form (fast mode);
+//  * adjoint(x, g): value and hand-derived reverse-mode gradient in one
+//    sweep (fast mode, ZEUS_GRAD_ADJOINT).
+// Objective data (Gaussian C, NLL bins) is held as device pointers: the
+// functor is trivially copyable, so it can sit in kernel parameters, CUDA
+// graphs and persistent kernels without the host-side deep copies the
+// reference's Matrix members imply (matrix.hpp:65-89).
+#pragma once
+
+#include <array>
+#include <cmath>
+#include <cstddef>
+#include <type_traits>
+
+#include "zb_dual.cuh"
+
+namespace zeus {
+
+  inline constexpr double kTwoPi = 2.0 * 3.14159265358979323846;
+
+  template <std::size_t D>
+  struct Rosenbrock {
+    static constexpr std::size_t arity = D;
+    static constexpr int kind = 0;
+
+    template <class T>
+    __host__ __device__ T
+    operator()(const std::array<T, D>& x) const
+    {
+      if constexpr (std::is_same_v<T, double>) {
+        double sum = 0.0;
+        for (std::size_t i = 0; i + 1 < D; ++i) {
+          const double t1 = 1.0 - x[i];
+          const double t2 = x[i + 1] - x[i] * x[i];
+          sum += t1 * t1 + 100.0 * t2 * t2;
+        }
+        return sum;
+      } else {
+        T sum(0.0, 0.0);
+        for (std::size_t i = 0; i + 1 < D; ++i) {
+          const T t1 = T(1.0, 0.0) - x[i];
+          const T t2 = x[i + 1] - x[i] * x[i];
+          sum = sum + t1 * t1 + T(100.0, 0.0) * t2 * t2;
+        }
+        return sum;
+      }
+    }
+
+    __host__ __device__ double
+    value(const double* x) const
+    {
+      double sum = 0.0;
+#pragma unroll 4
+      for (std::size_t i = 0; i + 1 < D; ++i) {
+        const double t1 = 1.0 - x[i];
+        const double t2 = fma(-x[i], x[i], x[i + 1]);
+        sum = fma(100.0 * t2, t2, fma(t1, t1, sum));
+      }
+      return sum;
+    }
+
+    // d/dx_i: -2(1-x_i) - 400 x_i (x_{i+1}-x_i^2) + 200 (x_i - x_{i-1}^2)
+    __host__ __device__ double
+    adjoint(const double* x, double* g) const
+    {
+      double sum = 0.0, carry = 0.0;
+#pragma unroll 4
+      for (std::size_t i = 0; i + 1 < D; ++i) {
+        const double t1 = 1.0 - x[i];
+        const double t2 = fma(-x[i], x[i], x[i + 1]);
+        sum = fma(100.0 * t2, t2, fma(t1, t1, sum));
+        g[i] = carry - 2.0 * t1 - 400.0 * x[i] * t2;
+        carry = 200.0 * t2;
+      }
+      g[D - 1] = carry;
+      return sum;
+    }
+  };
+
+  template <std::size_t D>
+  struct Rastrigin {
+    static constexpr std::size_t arity = D;
+    static constexpr int kind = 1;
+
+    template <class T>
+    __host__ __device__ T
+    operator()(const std::array<T, D>& x) const
+    {
+      if constexpr (std::is_same_v<T, double>) {
+        double sum = 10.0 * D;
+        for (std::size_t i = 0; i < D; ++i)
+          sum += x[i] * x[i] - 10.0 * ::cos(kTwoPi * x[i]);
+        return sum;
+      } else {
+        T sum(10.0 * D, 0.0);
+        for (std::size_t i = 0; i < D; ++i)
+          sum = sum + (x[i] * x[i] -
+                       T(10.0, 0.0) * dual::cos(x[i] * T(kTwoPi, 0.0)));
+        return sum;
+      }
+    }
+
+    __host__ __device__ double
+    value(const double* x) const
+    {
+      double sum = 10.0 * D;
+      for (std::size_t i = 0; i < D; ++i)
+        sum += fma(x[i], x[i], -10.0 * ::cospi(2.0 * x[i]));
+      return sum;
+    }
+
+    // d/dx_i: 2 x_i + 20 pi sin(2 pi x_i)
+    __host__ __device__ double
+    adjoint(const double* x, double* g) const
+    {
+      double sum = 10.0 * D;
+      for (std::size_t i = 0; i < D; ++i) {
+        double s, c;
+        ::sincospi(2.0 * x[i], &s, &c);
+        sum += fma(x[i], x[i], -10.0 * c);
+        g[i] = fma(10.0 * kTwoPi, s, 2.0 * x[i]);
+      }
+      return sum;
+    }
+  };
+
+  template <std::size_t D>
+  struct Ackley {
+    static constexpr std::size_t arity = D;
+    static constexpr int kind = 2;
+
+    template <class T>
+    __host__ __device__ T
+    operator()(const std::array<T, D>& x) const
+    {
+      if constexpr (std::is_same_v<T, double>) {
+        double sum_sq = 0.0, sum_cos = 0.0;
+        for (std::size_t i = 0; i < D; ++i) {
+          sum_sq += x[i] * x[i];
+          sum_cos += ::cos(kTwoPi * x[i]);
+        }
+        const double term1 = -20.0 * ::exp(-0.2 * ::sqrt(sum_sq / D));
+        const double term2 = -::exp(sum_cos / D);
+        return term1 + term2 + 20.0 + ::exp(1.0);
+      } else {
+        T sum_sq = 0.0, sum_cos = 0.0;
+        for (std::size_t i = 0; i < D; ++i) {
+          sum_sq += dual::pow(x[i], 2.0);
+          sum_cos += dual::cos(kTwoPi * x[i]);
+        }
+        const T term1 =
+          T(-20.0) * dual::exp(-0.2 * dual::sqrt(sum_sq / T(double(D))));
+        const T term2 = T(0.0) - dual::exp(sum_cos / T(double(D)));
+        return term1 + term2 + T(20.0) + dual::exp(T(1.0));
+      }
+    }
+
+    __host__ __device__ double
+    value(const double* x) const
+    {
+      double ss = 0.0, sc = 0.0;
+      for (std::size_t i = 0; i < D; ++i) {
+        ss = fma(x[i], x[i], ss);
+        sc += ::cospi(2.0 * x[i]);
+      }
+      constexpr double inv = 1.0 / double(D);
+      return -20.0 * ::exp(-0.2 * ::sqrt(ss * inv)) - ::exp(sc * inv) + 20.0 +
+             2.718281828459045;
+    }
+
+    // d/dx_i: 4 e^{-0.2 r} x_i / (D r) + (2 pi / D) e^{C/D} sin(2 pi x_i),
+    // r = sqrt(sum x^2 / D); NaN at r = 0 like the dual form.
+    __host__ __device__ double
+    adjoint(const double* x, double* g) const
+    {
+      double ss = 0.0, sc = 0.0;
+      for (std::size_t i = 0; i < D; ++i) {
+        double s, c;
+        ::sincospi(2.0 * x[i], &s, &c);
+        ss = fma(x[i], x[i], ss);
+        sc += c;
+        g[i] = s;
+      }
+      constexpr double inv = 1.0 / double(D);
+      const double r = ::sqrt(ss * inv);
+      const double e1 = ::exp(-0.2 * r), e2 = ::exp(sc * inv);
+      const double a = 4.0 * e1 * inv / r, b = kTwoPi * e2 * inv;
+      for (std::size_t i = 0; i < D; ++i)
+        g[i] = fma(a, x[i], b * g[i]);
+      return -20.0 * e1 - e2 + 20.0 + 2.718281828459045;
+    }
+  };
+
+  // 0.5 x^T C x with C a dense D x D row-major device matrix.
+  template <std::size_t D>
+  struct Gaussian {
+    static constexpr std::size_t arity = D;
+    static constexpr int kind = 3;
+    const double* C = nullptr; // device pointer, D*D
+    bool symmetric = true;     // checked on the host when built from data
+
+    template <class T>
+    __host__ __device__ T
+    operator()(const std::array<T, D>& x) const
+    {
+      const double* Cp = C;
+      T q = T(0);
+      for (std::size_t i = 0; i < D; ++i)
+        for (std::size_t j = 0; j < D; ++j)
+          q += x[i] * T(Cp[i * D + j]) * x[j];
+      return T(0.5) * q;
+    }
+
+    __host__ __device__ double
+    value(const double* x) const
+    {
+      double q = 0.0;
+      for (std::size_t i = 0; i < D; ++i) {
+        double r = 0.0;
+        for (std::size_t j = 0; j < D; ++j)
+          r = fma(C[i * D + j], x[j], r);
+        q = fma(x[i], r, q);
+      }
+      return 0.5 * q;
+    }
+
+    // grad = (C + C^T) x / 2 (= C x when C is symmetric)
+    __host__ __device__ double
+    adjoint(const double* x, double* g) const
+    {
+      double q = 0.0;
+      for (std::size_t i = 0; i < D; ++i) {
+        double r = 0.0;
+        for (std::size_t j = 0; j < D; ++j)
+          r = fma(C[i * D + j], x[j], r);
+        g[i] = r;
+        q = fma(x[i], r, q);
+      }
+      if (!symmetric) {
+        for (std::size_t i = 0; i < D; ++i) {
+          double c = 0.0;
+          for (std::size_t j = 0; j < D; ++j)
+            c = fma(C[j * D + i], x[j], c);
+          g[i] = 0.5 * (g[i] + c);
+        }
+      }
+      return 0.5 * q;
+    }
+  };
+
+  // Binned Poisson negative log-likelihood of the dijet shape
+  // lambda_i = a (1-x_i)^b / x_i^(c + d ln x_i) (LogLikelihood.h:29-58).
+  // `bins` holds per-bin constants for the fast paths, 4 doubles per bin:
+  // {ln x_i, ln(1 - x_i), k_i, lgamma(k_i + 1)}; centres/counts feed the
+  // reference-order operator().
+  struct PoissonNLL {
+    static constexpr std::size_t arity = 4;
+    static constexpr int kind = 4;
+    const double* centres = nullptr;
+    const int* counts = nullptr;
+    const double* bins = nullptr;
+    int nbins = 0;
+
+    template <class T>
+    __host__ __device__ T
+    operator()(const std::array<T, 4>& th) const
+    {
+      using ::lgamma;
+      using ::log;
+      using ::pow;
+      const T a = th[0], b = th[1], c = th[2], d = th[3];
+      T nll = T(0);
+      for (int i = 0; i < nbins; ++i) {
+        const T x = T(centres[i]);
+        const int ki = counts[i];
+        const T mean = a * pow(T(1.0) - x, b) / pow(x, c + d * log(x));
+        const T log_p = T(ki) * log(mean) - mean - lgamma(T(ki) + T(1));
+        nll -= log_p;
+      }
+      return nll;
+    }
+
+    // ln lambda = ln a + b ln(1-x) - (c + d ln x) ln x
+    __host__ __device__ double
+    value(const double* th) const
+    {
+      const double la = ::log(th[0]);
+      double nll = 0.0;
+      for (int i = 0; i < nbins; ++i) {
+        const double lx = bins[4 * i], l1 = bins[4 * i + 1];
+        const double k = bins[4 * i + 2], lgk = bins[4 * i + 3];
+        const double ll = la + fma(th[1], l1, -fma(th[3], lx, th[2]) * lx);
+        nll += ::exp(ll) - fma(k, ll, -lgk);
+      }
+      return nll;
+    }
+
+    // dNLL/dtheta = sum (lambda - k) dln(lambda)/dtheta with
+    // dln(lambda) = (1/a, ln(1-x), -ln x, -(ln x)^2)
+    __host__ __device__ double
+    adjoint(const double* th, double* g) const
+    {
+      const double la = ::log(th[0]);
+      double nll = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0, g3 = 0.0;
+      for (int i = 0; i < nbins; ++i) {
+        const double lx = bins[4 * i], l1 = bins[4 * i + 1];
+        const double k = bins[4 * i + 2], lgk = bins[4 * i + 3];
+        const double ll = la + fma(th[1], l1, -fma(th[3], lx, th[2]) * lx);
+        const double lam = ::exp(ll);
+        nll += lam - fma(k, ll, -lgk);
+        const double w = lam - k;
+        g0 += w;
+        g1 = fma(w, l1, g1);
+        g2 = fma(-w, lx, g2);
+        g3 = fma(-w * lx, lx, g3);
+      }
+      g[0] = g0 / th[0];
+      g[1] = g1;
+      g[2] = g2;
+      g[3] = g3;
+      return nll;
+    }
+  };
+
+} // namespace zeus

@@ -1,0 +1,699 @@
+// C ABI (include/zeus_b200.h): validation, workspace layout, PSO graph
+// capture, reductions and the host-buffer orchestration of zeus_optimize.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "zb_internal.h"
+#include "zb_objective_visit.cuh"
+#include "zb_philox.cuh"
+#include "zb_reduce.cuh"
+
+namespace zb {
+
+  namespace {
+    thread_local char g_err[1024] = "";
+  }
+
+  void
+  set_error(const char* fmt, ...)
+  {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+  }
+
+  int
+  cuda_fail(cudaError_t e, const char* what)
+  {
+    if (e == cudaSuccess)
+      return ZEUS_OK;
+    set_error("%s: %s", what, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? ZEUS_E_NOMEM : ZEUS_E_CUDA;
+  }
+
+  int
+  sm_count()
+  {
+    static std::mutex mu;
+    static std::map<int, int> cache;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+      return 148;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(dev);
+    if (it != cache.end())
+      return it->second;
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) !=
+          cudaSuccess ||
+        v <= 0)
+      v = 148;
+    cache[dev] = v;
+    return v;
+  }
+
+  __global__ void __launch_bounds__(1024)
+    census_kernel(const double* __restrict__ fval,
+                  const int32_t* __restrict__ status,
+                  const double* __restrict__ x, int64_t n, int dim,
+                  KnownMin km, Census* out)
+  {
+    __shared__ int cnt[4];
+    if (threadIdx.x < 4)
+      cnt[threadIdx.x] = 0;
+    __syncthreads();
+    unsigned long long key = ~0ull;
+    int idx = 0x7fffffff;
+    int actual = 0, claimed = 0, stopped = 0, surr = 0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+      const unsigned long long k = order_key(fval[i]);
+      if (k < key || (k == key && (int)i < idx)) {
+        key = k;
+        idx = (int)i;
+      }
+      const int st = status[i];
+      if (st == kConverged) {
+        ++claimed;
+        if (x) {
+          double ss = 0.0;
+          for (int d = 0; d < dim; ++d) {
+            const double m = km.has ? km.x[d] : 0.0;
+            const double df = x[i * dim + d] - m;
+            ss += df * df;
+          }
+          if (sqrt(ss) < 0.5)
+            ++actual;
+        }
+      } else if (st == kStopped) {
+        ++stopped;
+      } else {
+        ++surr;
+      }
+    }
+    atomicAdd(&cnt[0], actual);
+    atomicAdd(&cnt[1], claimed);
+    atomicAdd(&cnt[2], surr);
+    atomicAdd(&cnt[3], stopped);
+    block_argmin(key, idx);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      out->actual = cnt[0];
+      out->claimed = cnt[1];
+      out->surrendered = cnt[2];
+      out->stopped = cnt[3];
+      out->best_idx = (n > 0 && idx != 0x7fffffff) ? idx : -1;
+      out->reserved = 0;
+    }
+  }
+
+  __global__ void
+  nll_bins_kernel(const double* __restrict__ centres,
+                  const int* __restrict__ counts, int nbins,
+                  double* __restrict__ bins)
+  {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nbins)
+      return;
+    const double x = centres[i];
+    const double k = (double)counts[i];
+    bins[4 * i + 0] = ::log(x);
+    bins[4 * i + 1] = ::log(1.0 - x);
+    bins[4 * i + 2] = k;
+    bins[4 * i + 3] = ::lgamma(k + 1.0);
+  }
+
+  __global__ void
+  starts_kernel(uint64_t seed, int64_t n, int dim, double lower, double upper,
+                double* __restrict__ out)
+  {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * dim)
+      return;
+    const int64_t i = e / dim;
+    const int d = (int)(e - i * dim);
+    out[e] =
+      lower + (upper - lower) * uniform01(seed, kTagStarts, (uint64_t)i, d);
+  }
+
+  __global__ void __launch_bounds__(256)
+    fp64_probe_kernel(int64_t iters, double* __restrict__ sink)
+  {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    double a0 = 1.0 + t * 1e-9, a1 = a0 + 1e-3, a2 = a0 + 2e-3, a3 = a0 + 3e-3;
+    double a4 = a0 + 4e-3, a5 = a0 + 5e-3, a6 = a0 + 6e-3, a7 = a0 + 7e-3;
+    const double m = 0.999999999, c = 1e-9;
+    for (int64_t i = 0; i < iters; ++i) {
+      a0 = fma(a0, m, c);
+      a1 = fma(a1, m, c);
+      a2 = fma(a2, m, c);
+      a3 = fma(a3, m, c);
+      a4 = fma(a4, m, c);
+      a5 = fma(a5, m, c);
+      a6 = fma(a6, m, c);
+      a7 = fma(a7, m, c);
+    }
+    sink[t] = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  }
+
+  namespace {
+
+    int
+    check_problem(const zeus_problem* p)
+    {
+      if (!p) {
+        set_error("problem is NULL");
+        return ZEUS_E_INVALID;
+      }
+      if (!builtin_supported(p->kind, p->dim)) {
+        set_error("objective kind %d with dim %d is not built", p->kind,
+                  p->dim);
+        return ZEUS_E_UNSUPPORTED;
+      }
+      if (p->kind == ZEUS_OBJ_GAUSSIAN && !p->data) {
+        set_error("Gaussian objective needs its matrix (data)");
+        return ZEUS_E_INVALID;
+      }
+      if (p->kind == ZEUS_OBJ_POISSON_NLL &&
+          (!p->data || !p->idata || p->ndata <= 0)) {
+        set_error("Poisson NLL needs centres, counts and ndata > 0");
+        return ZEUS_E_INVALID;
+      }
+      return ZEUS_OK;
+    }
+
+    Objective
+    to_objective(const zeus_problem* p, const double* nll_bins)
+    {
+      Objective o;
+      o.kind = p->kind;
+      o.dim = p->dim;
+      o.data = p->data;
+      o.idata = p->idata;
+      o.ndata = p->ndata;
+      o.flags = p->flags;
+      o.nll_bins = nll_bins;
+      return o;
+    }
+
+    size_t
+    nll_bytes(const zeus_problem* p)
+    {
+      return p->kind == ZEUS_OBJ_POISSON_NLL
+               ? align_up(sizeof(double) * 4 * (size_t)p->ndata)
+               : 0;
+    }
+
+    int
+    check_config(const zeus_bfgs_config* c)
+    {
+      if (!c) {
+        set_error("config is NULL");
+        return ZEUS_E_INVALID;
+      }
+      if (c->max_iter < 0) {
+        set_error("max_iter must be >= 0");
+        return ZEUS_E_INVALID;
+      }
+      if (c->mode != ZEUS_MODE_EXACT && c->mode != ZEUS_MODE_FAST) {
+        set_error("unknown mode %d", c->mode);
+        return ZEUS_E_INVALID;
+      }
+      if (c->gradient != ZEUS_GRAD_DUAL && c->gradient != ZEUS_GRAD_ADJOINT) {
+        set_error("unknown gradient %d", c->gradient);
+        return ZEUS_E_INVALID;
+      }
+      if (c->mode == ZEUS_MODE_EXACT && c->gradient != ZEUS_GRAD_DUAL) {
+        set_error("exact mode uses dual gradients only");
+        return ZEUS_E_INVALID;
+      }
+      if (!(c->tolerance >= 0.0)) {
+        set_error("tolerance must be >= 0");
+        return ZEUS_E_INVALID;
+      }
+      return ZEUS_OK;
+    }
+
+    size_t
+    kernel_ws(const zeus_problem* p, const zeus_bfgs_config* c, int64_t n)
+    {
+      Objective o = to_objective(p, nullptr);
+      return c->mode == ZEUS_MODE_EXACT ? exact_workspace_bytes(o, n)
+                                        : fast_workspace_bytes(o, *c, n);
+    }
+
+    // Cached executable graphs for the PSO loop, keyed by the launch shape;
+    // new pointer arguments go in through cudaGraphExecUpdate.
+    struct GraphCache {
+      std::mutex mu;
+      std::map<std::tuple<int, int, int, int64_t, int>, cudaGraphExec_t> m;
+    };
+    GraphCache&
+    graph_cache()
+    {
+      static GraphCache* c = new GraphCache; // never destroyed: exit-safe
+      return *c;
+    }
+
+  } // namespace
+} // namespace zb
+
+using namespace zb;
+
+extern "C" {
+
+const char*
+zeus_last_error(void)
+{
+  return g_err;
+}
+
+const char*
+zeus_version(void)
+{
+  return "zeus_b200 0.1.0 (sm_100a)";
+}
+
+int
+zeus_supported(int32_t kind, int32_t dim, int32_t mode, int32_t gradient)
+{
+  if (mode == ZEUS_MODE_EXACT)
+    return gradient == ZEUS_GRAD_DUAL && exact_supported(kind, dim);
+  if (mode == ZEUS_MODE_FAST)
+    return fast_supported(kind, dim, gradient);
+  return 0;
+}
+
+int
+zeus_starts_uniform(uint64_t seed, int64_t n, int32_t dim, double lower,
+                    double upper, double* d_out, void* stream)
+{
+  if (n < 0 || dim <= 0 || (n > 0 && !d_out)) {
+    set_error("zeus_starts_uniform: bad arguments");
+    return ZEUS_E_INVALID;
+  }
+  if (n == 0)
+    return ZEUS_OK;
+  const int64_t total = n * dim;
+  const unsigned grid = (unsigned)((total + 255) / 256);
+  starts_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(seed, n, dim, lower,
+                                                       upper, d_out);
+  return cuda_fail(cudaGetLastError(), "starts launch");
+}
+
+size_t
+zeus_pso_workspace_size(int64_t n, int32_t dim)
+{
+  if (n <= 0 || dim <= 0)
+    return 0;
+  return pso_workspace_bytes(n, dim);
+}
+
+int
+zeus_pso_device(const zeus_problem* problem, uint64_t seed, int64_t n,
+                double lower, double upper, int32_t iters, double w,
+                double c1, double c2, double* d_pbest_x, double* d_pbest_f,
+                double* d_gbest, void* d_workspace, size_t workspace_bytes,
+                void* stream)
+{
+  int rc = check_problem(problem);
+  if (rc)
+    return rc;
+  if (n < 0 || iters < 0 || (n > 0 && (!d_pbest_x || !d_pbest_f || !d_gbest))) {
+    set_error("zeus_pso_device: bad arguments");
+    return ZEUS_E_INVALID;
+  }
+  if (n == 0)
+    return ZEUS_OK;
+  if (n > 0x7fffffffLL) {
+    set_error("zeus_pso_device: n must fit in int32");
+    return ZEUS_E_INVALID;
+  }
+  Objective o = to_objective(problem, nullptr);
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (st)
+    cudaStreamIsCapturing(st, &cs);
+  if (!st || cs != cudaStreamCaptureStatusNone)
+    return launch_pso(o, seed, n, lower, upper, iters, w, c1, c2, d_pbest_x,
+                      d_pbest_f, d_gbest, d_workspace, workspace_bytes, st);
+  // Capture init + iterations into one graph and launch it.
+  rc = cuda_fail(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal),
+                 "PSO capture begin");
+  if (rc)
+    return rc;
+  const int lrc =
+    launch_pso(o, seed, n, lower, upper, iters, w, c1, c2, d_pbest_x,
+               d_pbest_f, d_gbest, d_workspace, workspace_bytes, st);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+  if (lrc) {
+    if (graph)
+      cudaGraphDestroy(graph);
+    return lrc;
+  }
+  if ((rc = cuda_fail(ec, "PSO capture end")))
+    return rc;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  auto key = std::make_tuple(dev, o.kind, o.dim, n, (int)iters);
+  GraphCache& gc = graph_cache();
+  std::lock_guard<std::mutex> lk(gc.mu);
+  cudaGraphExec_t exec = nullptr;
+  auto it = gc.m.find(key);
+  if (it != gc.m.end()) {
+    cudaGraphExecUpdateResultInfo info;
+    if (cudaGraphExecUpdate(it->second, graph, &info) == cudaSuccess)
+      exec = it->second;
+    else {
+      cudaGetLastError();
+      cudaStreamSynchronize(st);
+      cudaGraphExecDestroy(it->second);
+      gc.m.erase(it);
+    }
+  }
+  if (!exec) {
+    rc = cuda_fail(cudaGraphInstantiate(&exec, graph, 0), "PSO graph");
+    if (rc) {
+      cudaGraphDestroy(graph);
+      return rc;
+    }
+    gc.m[key] = exec;
+  }
+  cudaGraphDestroy(graph);
+  return cuda_fail(cudaGraphLaunch(exec, st), "PSO graph launch");
+}
+
+size_t
+zeus_bfgs_workspace_size(const zeus_problem* problem,
+                         const zeus_bfgs_config* config, int64_t n)
+{
+  if (check_problem(problem) || check_config(config) || n <= 0)
+    return 0;
+  return nll_bytes(problem) + align_up(kernel_ws(problem, config, n));
+}
+
+int
+zeus_bfgs_device(const zeus_problem* problem, const zeus_bfgs_config* config,
+                 const double* d_starts, int64_t n,
+                 const zeus_run_outputs* out, int32_t* d_control,
+                 void* d_workspace, size_t workspace_bytes, void* stream)
+{
+  int rc = check_problem(problem);
+  if (rc)
+    return rc;
+  if ((rc = check_config(config)))
+    return rc;
+  if (n < 0 || n > 0x7fffffffLL || !out || (n > 0 && (!d_starts || !d_control))) {
+    set_error("zeus_bfgs_device: bad arguments");
+    return ZEUS_E_INVALID;
+  }
+  if (n == 0)
+    return ZEUS_OK;
+  if (config->mode == ZEUS_MODE_FAST &&
+      !fast_supported(problem->kind, problem->dim, config->gradient)) {
+    set_error("fast mode: kind %d dim %d not built", problem->kind,
+              problem->dim);
+    return ZEUS_E_UNSUPPORTED;
+  }
+  const size_t need = zeus_bfgs_workspace_size(problem, config, n);
+  if (need > 0 && (!d_workspace || workspace_bytes < need)) {
+    set_error("zeus_bfgs_device: workspace of %zu bytes needed, got %zu",
+              need, workspace_bytes);
+    return ZEUS_E_WORKSPACE;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  char* ws = static_cast<char*>(d_workspace);
+  const double* bins = nullptr;
+  if (problem->kind == ZEUS_OBJ_POISSON_NLL) {
+    double* b = reinterpret_cast<double*>(ws);
+    nll_bins_kernel<<<(problem->ndata + 127) / 128, 128, 0, st>>>(
+      problem->data, problem->idata, problem->ndata, b);
+    if ((rc = cuda_fail(cudaGetLastError(), "NLL bins launch")))
+      return rc;
+    bins = b;
+    ws += nll_bytes(problem);
+  }
+  const size_t kws = need - nll_bytes(problem);
+  Objective o = to_objective(problem, bins);
+  BfgsParams prm{n, config->max_iter, config->required_converged,
+                 config->tolerance};
+  RunOut ro{out->fval,     out->status, out->iter,   out->gnorm,
+            out->x,        out->counters, out->traj_x, out->traj_f,
+            out->traj_g,   out->traj_status};
+  Control* ctl = reinterpret_cast<Control*>(d_control);
+  if (config->mode == ZEUS_MODE_EXACT)
+    return launch_exact(o, prm, d_starts, ro, ctl, ws, kws, st);
+  return launch_fast(o, *config, prm, d_starts, ro, ctl, ws, kws, st);
+}
+
+int
+zeus_census_device(const double* d_fval, const int32_t* d_status,
+                   const double* d_x, int64_t n, int32_t dim,
+                   const double* known_min, zeus_census* d_census,
+                   void* stream)
+{
+  if (n < 0 || !d_census || (n > 0 && (!d_fval || !d_status)) || dim <= 0 ||
+      (known_min && dim > kMaxKnownDim)) {
+    set_error("zeus_census_device: bad arguments");
+    return ZEUS_E_INVALID;
+  }
+  KnownMin km;
+  km.has = known_min ? 1 : 0;
+  for (int d = 0; d < kMaxKnownDim; ++d)
+    km.x[d] = (known_min && d < dim) ? known_min[d] : 0.0;
+  census_kernel<<<1, 1024, 0, (cudaStream_t)stream>>>(
+    d_fval, d_status, d_x, n, dim, km, reinterpret_cast<Census*>(d_census));
+  return cuda_fail(cudaGetLastError(), "census launch");
+}
+
+int
+zeus_optimize(const zeus_problem* hp, double lower, double upper, int64_t n,
+              int32_t max_iter, int32_t pso_iter, int32_t required_converged,
+              double tolerance, uint64_t seed, const zeus_bfgs_config* config,
+              zeus_result* best, double* best_x, zeus_census* census,
+              double* per_run_fval, int32_t* per_run_status, void* stream)
+{
+  if (!best) {
+    set_error("zeus_optimize: best is NULL");
+    return ZEUS_E_INVALID;
+  }
+  *best = zeus_result{-1, -1, 37.0, 0.0, 0, 0}; // util.hpp:36-54 defaults
+  if (census)
+    *census = zeus_census{0, 0, 0, 0, -1, 0};
+  int rc = check_problem(hp);
+  if (rc)
+    return rc;
+  zeus_bfgs_config cfg;
+  if (config)
+    cfg = *config;
+  else {
+    cfg = zeus_bfgs_config{};
+    cfg.mode = ZEUS_MODE_FAST;
+    cfg.gradient = ZEUS_GRAD_ADJOINT;
+  }
+  cfg.max_iter = max_iter;
+  cfg.required_converged = required_converged;
+  cfg.tolerance = tolerance;
+  if ((rc = check_config(&cfg)))
+    return rc;
+  if (n < 0) {
+    set_error("zeus_optimize: n < 0");
+    return ZEUS_E_INVALID;
+  }
+  if (n == 0) // zeus.cuh:58-60: N == 0 returns the default Result
+    return ZEUS_OK;
+  const int dim = hp->dim;
+  cudaStream_t st = (cudaStream_t)stream;
+
+  std::vector<void*> allocs;
+  auto fail = [&](int code) {
+    for (void* p : allocs)
+      cudaFreeAsync(p, st);
+    cudaStreamSynchronize(st);
+    best->status = (code == ZEUS_E_NOMEM) ? ZEUS_STATUS_NOMEM
+                                          : ZEUS_STATUS_KERNEL;
+    return code;
+  };
+  auto alloc = [&](size_t bytes, void** out) -> int {
+    *out = nullptr;
+    if (bytes == 0)
+      return ZEUS_OK;
+    const int r = cuda_fail(cudaMallocAsync(out, bytes, st), "allocation");
+    if (r == ZEUS_OK)
+      allocs.push_back(*out);
+    return r;
+  };
+
+  // problem data to the device
+  zeus_problem dp = *hp;
+  if (hp->kind == ZEUS_OBJ_GAUSSIAN) {
+    void* c = nullptr;
+    const size_t b = sizeof(double) * (size_t)dim * dim;
+    if ((rc = alloc(b, &c)))
+      return fail(rc);
+    if ((rc = cuda_fail(cudaMemcpyAsync(c, hp->data, b,
+                                        cudaMemcpyHostToDevice, st),
+                        "H2D problem data")))
+      return fail(rc);
+    bool symmetric = true;
+    for (int i = 0; i < dim && symmetric; ++i)
+      for (int j = i + 1; j < dim; ++j)
+        if (hp->data[(size_t)i * dim + j] != hp->data[(size_t)j * dim + i]) {
+          symmetric = false;
+          break;
+        }
+    dp.data = static_cast<const double*>(c);
+    dp.flags = symmetric ? ZEUS_PROBLEM_SYMMETRIC : 0;
+  } else if (hp->kind == ZEUS_OBJ_POISSON_NLL) {
+    void *c = nullptr, *k = nullptr;
+    if ((rc = alloc(sizeof(double) * hp->ndata, &c)) ||
+        (rc = alloc(sizeof(int32_t) * hp->ndata, &k)))
+      return fail(rc);
+    if ((rc = cuda_fail(cudaMemcpyAsync(c, hp->data,
+                                        sizeof(double) * hp->ndata,
+                                        cudaMemcpyHostToDevice, st),
+                        "H2D centres")) ||
+        (rc = cuda_fail(cudaMemcpyAsync(k, hp->idata,
+                                        sizeof(int32_t) * hp->ndata,
+                                        cudaMemcpyHostToDevice, st),
+                        "H2D counts")))
+      return fail(rc);
+    dp.data = static_cast<const double*>(c);
+    dp.idata = static_cast<const int32_t*>(k);
+  }
+
+  void *starts, *pbf, *gbest, *pso_ws, *fval, *status, *iters, *gnorm, *xo,
+    *ctl, *cen, *bws;
+  const size_t nd = (size_t)n * dim;
+  if ((rc = alloc(sizeof(double) * nd, &starts)) ||
+      (rc = alloc(sizeof(double) * n, &fval)) ||
+      (rc = alloc(sizeof(int32_t) * n, &status)) ||
+      (rc = alloc(sizeof(int32_t) * n, &iters)) ||
+      (rc = alloc(sizeof(double) * n, &gnorm)) ||
+      (rc = alloc(sizeof(double) * nd, &xo)) ||
+      (rc = alloc(sizeof(int32_t) * 2, &ctl)) ||
+      (rc = alloc(sizeof(zeus_census), &cen)))
+    return fail(rc);
+  if (pso_iter >= 0) {
+    const size_t pws = zeus_pso_workspace_size(n, dim);
+    if ((rc = alloc(sizeof(double) * n, &pbf)) ||
+        (rc = alloc(sizeof(double) * (dim + 1), &gbest)) ||
+        (rc = alloc(pws, &pso_ws)))
+      return fail(rc);
+    if ((rc = zeus_pso_device(&dp, seed, n, lower, upper, pso_iter, 0.5, 1.2,
+                              1.5, static_cast<double*>(starts),
+                              static_cast<double*>(pbf),
+                              static_cast<double*>(gbest), pso_ws, pws, st)))
+      return fail(rc);
+  } else {
+    if ((rc = zeus_starts_uniform(seed, n, dim, lower, upper,
+                                  static_cast<double*>(starts), st)))
+      return fail(rc);
+  }
+  const size_t bw = zeus_bfgs_workspace_size(&dp, &cfg, n);
+  if ((rc = alloc(bw, &bws)))
+    return fail(rc);
+  if ((rc = cuda_fail(cudaMemsetAsync(ctl, 0, sizeof(int32_t) * 2, st),
+                      "control reset")))
+    return fail(rc);
+  zeus_run_outputs ro{};
+  ro.fval = static_cast<double*>(fval);
+  ro.status = static_cast<int32_t*>(status);
+  ro.iter = static_cast<int32_t*>(iters);
+  ro.gnorm = static_cast<double*>(gnorm);
+  ro.x = static_cast<double*>(xo);
+  if ((rc = zeus_bfgs_device(&dp, &cfg, static_cast<double*>(starts), n, &ro,
+                             static_cast<int32_t*>(ctl), bws, bw, st)))
+    return fail(rc);
+  std::vector<double> km;
+  if (hp->kind == ZEUS_OBJ_ROSENBROCK)
+    km.assign(dim, 1.0);
+  if ((rc = zeus_census_device(ro.fval, ro.status, ro.x, n, dim,
+                               km.empty() ? nullptr : km.data(),
+                               static_cast<zeus_census*>(cen), st)))
+    return fail(rc);
+  zeus_census hc;
+  if ((rc = cuda_fail(cudaMemcpyAsync(&hc, cen, sizeof hc,
+                                      cudaMemcpyDeviceToHost, st),
+                      "D2H census")) ||
+      (rc = cuda_fail(cudaStreamSynchronize(st), "BFGS run")))
+    return fail(rc);
+  if (census)
+    *census = hc;
+  if (hc.best_idx >= 0) {
+    const int b = hc.best_idx;
+    int32_t bst = 0, bit = 0;
+    double bf = 0.0, bg = 0.0;
+    if ((rc = cuda_fail(cudaMemcpyAsync(&bf, ro.fval + b, sizeof bf,
+                                        cudaMemcpyDeviceToHost, st),
+                        "D2H best")) ||
+        (rc = cuda_fail(cudaMemcpyAsync(&bst, ro.status + b, sizeof bst,
+                                        cudaMemcpyDeviceToHost, st),
+                        "D2H best")) ||
+        (rc = cuda_fail(cudaMemcpyAsync(&bit, ro.iter + b, sizeof bit,
+                                        cudaMemcpyDeviceToHost, st),
+                        "D2H best")) ||
+        (rc = cuda_fail(cudaMemcpyAsync(&bg, ro.gnorm + b, sizeof bg,
+                                        cudaMemcpyDeviceToHost, st),
+                        "D2H best")))
+      return fail(rc);
+    if (best_x &&
+        (rc = cuda_fail(cudaMemcpyAsync(best_x, ro.x + (size_t)b * dim,
+                                        sizeof(double) * dim,
+                                        cudaMemcpyDeviceToHost, st),
+                        "D2H best x")))
+      return fail(rc);
+    if (per_run_fval &&
+        (rc = cuda_fail(cudaMemcpyAsync(per_run_fval, ro.fval,
+                                        sizeof(double) * n,
+                                        cudaMemcpyDeviceToHost, st),
+                        "D2H fvals")))
+      return fail(rc);
+    if (per_run_status &&
+        (rc = cuda_fail(cudaMemcpyAsync(per_run_status, ro.status,
+                                        sizeof(int32_t) * n,
+                                        cudaMemcpyDeviceToHost, st),
+                        "D2H statuses")))
+      return fail(rc);
+    if ((rc = cuda_fail(cudaStreamSynchronize(st), "D2H sync")))
+      return fail(rc);
+    best->idx = b;
+    best->status = bst;
+    best->fval = bf;
+    best->gradient_norm = bg;
+    best->iter = bit;
+  }
+  for (void* p : allocs)
+    cudaFreeAsync(p, st);
+  return cuda_fail(cudaStreamSynchronize(st), "free");
+}
+
+void
+zeus_probe_fp64_shape(int32_t* grid, int32_t* block)
+{
+  if (grid)
+    *grid = sm_count() * 8;
+  if (block)
+    *block = 256;
+}
+
+int
+zeus_probe_fp64(int64_t iters, double* d_sink, void* stream)
+{
+  if (iters < 0 || !d_sink) {
+    set_error("zeus_probe_fp64: bad arguments");
+    return ZEUS_E_INVALID;
+  }
+  fp64_probe_kernel<<<sm_count() * 8, 256, 0, (cudaStream_t)stream>>>(iters,
+                                                                       d_sink);
+  return cuda_fail(cudaGetLastError(), "FP64 probe launch");
+}
+
+} // extern "C"
