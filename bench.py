@@ -210,7 +210,10 @@ def run_gpu(args, rank, world, local_rank):
     wl = workloads()[args.workload]
     jobs = wl["jobs"]
     dev = torch.device("cuda", local_rank)
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-legacy) stream: the PSO loop is captured into a CUDA
+    # graph on it
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
     seed = args.seed + 1000003 * rank
 
