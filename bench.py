@@ -152,6 +152,11 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.rows.append([c.strip() for c in line.split(",")])
 
+    def wait_samples(self, n, timeout=3.0):
+        t0 = time.time()
+        while self.proc is not None and len(self.rows) < n and time.time() - t0 < timeout:
+            time.sleep(0.02)
+
     def stop(self):
         if self.proc is not None:
             self.proc.terminate()
@@ -274,6 +279,7 @@ def run_gpu(args, rank, world, local_rank):
     clocks = ClockSampler(local_rank)
     if rank == 0:
         clocks.start()
+        clocks.wait_samples(1)
     times, kern_ms, conv, launches = [], [], [], 0
     counters = []
     for k in range(args.steps):
@@ -294,6 +300,8 @@ def run_gpu(args, rank, world, local_rank):
         counters = [((s["obj"].kind, s["obj"].dim, args.gradient, s["nbins"]),
                      s["run"].counters.cpu().numpy()) for s in state]
     if rank == 0:
+        n0 = len(clocks.rows)
+        clocks.wait_samples(n0 + 1)  # one sample after the last timed step
         clocks.stop()
 
     step_ms = float(np.mean(times))
@@ -379,6 +387,23 @@ def run_gpu(args, rank, world, local_rank):
 
 
 # ---------------------------------------------------------------- CPU side
+class _QuietStdout:
+    """Silences C-level stdout (the reference's host build prints from its
+    convergence check) so this process prints only its JSON line."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+        return self
+
+    def __exit__(self, *exc):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
 def _ref_lib():
     from tests import _oracle as O
 
@@ -399,11 +424,12 @@ def cpu_baseline(args, state, torch):
     for s in state:
         j, obj = s["job"], s["obj"]
         starts = s["pso"]["pbx"].cpu().numpy()
-        t0 = time.perf_counter()
-        r = O.ref_bfgs(obj.kind, obj.dim, starts, max_iter=j.max_iter, required=j.required,
-                       tol=j.tol, data=obj.data, idata=obj.idata, lower=j.lo, upper=j.hi,
-                       nthreads=cores)
-        total_t += time.perf_counter() - t0
+        with _QuietStdout():
+            t0 = time.perf_counter()
+            r = O.ref_bfgs(obj.kind, obj.dim, starts, max_iter=j.max_iter,
+                           required=j.required, tol=j.tol, data=obj.data, idata=obj.idata,
+                           lower=j.lo, upper=j.hi, nthreads=cores)
+            total_t += time.perf_counter() - t0
         total_conv += int((r["status"] == 1).sum())
         sample.append(f"{j.name}: all {j.n} runs from the GPU's PSO starts")
     return {"value": total_conv / total_t, "unit": "runs/s", "cores": cores,
@@ -434,9 +460,10 @@ def run_reference(args, rank, world):
         t0 = time.perf_counter()
         c = 0
         for j, obj, pbx in sts:
-            r = O.ref_bfgs(obj.kind, obj.dim, pbx, max_iter=j.max_iter,
-                           required=j.required, tol=j.tol, data=obj.data, idata=obj.idata,
-                           lower=j.lo, upper=j.hi, nthreads=cores)
+            with _QuietStdout():
+                r = O.ref_bfgs(obj.kind, obj.dim, pbx, max_iter=j.max_iter,
+                               required=j.required, tol=j.tol, data=obj.data,
+                               idata=obj.idata, lower=j.lo, upper=j.hi, nthreads=cores)
             c += int((r["status"] == 1).sum())
         dt = time.perf_counter() - t0
         if k >= args.warmup:

@@ -65,6 +65,17 @@ extern "C" {
 #define ZEUS_GRAD_DUAL 0    /* D forward dual passes (duals.cuh:241-266) */
 #define ZEUS_GRAD_ADJOINT 1 /* hand-written reverse-mode gradient */
 
+/* zeus_bfgs_config.flags
+ * NO_FIXED_POINT: keep iterating a run whose iteration changed nothing.  By
+ *   default a run whose step was rejected (f_new >= best) AND whose update
+ *   was skipped (|s.y| < 1e-14) ends at once with status 0 and iter =
+ *   max_iter: its state (x, g, H, best) is unchanged, so every remaining
+ *   iteration would repeat it bit for bit and the reference would return
+ *   exactly that result at MAX_ITER (with stop-early on, it is the result the
+ *   reference gives when the run reaches MAX_ITER before the stop flag).
+ *   Trajectory recording always iterates to the end. */
+#define ZEUS_FLAG_NO_FIXED_POINT 1
+
 #define ZEUS_LAYOUT_AUTO 0
 #define ZEUS_LAYOUT_THREAD 1 /* one run per thread, H in registers */
 #define ZEUS_LAYOUT_TILE 2   /* one run per 2..32-lane tile, H rows per lane */
@@ -88,7 +99,7 @@ typedef struct zeus_bfgs_config {
   int32_t layout;             /* ZEUS_LAYOUT_* */
   int32_t tile;               /* lanes per run for TILE (0 = auto) */
   int32_t block;              /* threads per block (0 = auto) */
-  int32_t reserved;
+  int32_t flags;              /* ZEUS_FLAG_* */
 } zeus_bfgs_config;
 
 /* Per-run outputs, all device pointers; NULL members are not written.

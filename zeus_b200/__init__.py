@@ -31,6 +31,7 @@ PROBLEM_SYMMETRIC = 1
 MODE_EXACT, MODE_FAST = 0, 1
 GRAD_DUAL, GRAD_ADJOINT = 0, 1
 LAYOUT_AUTO, LAYOUT_THREAD, LAYOUT_TILE, LAYOUT_CTA = 0, 1, 2, 3
+FLAG_NO_FIXED_POINT = 1
 
 _MODES = {"exact": MODE_EXACT, "fast": MODE_FAST}
 _GRADS = {"dual": GRAD_DUAL, "adjoint": GRAD_ADJOINT}
@@ -65,7 +66,7 @@ class BfgsConfig(C.Structure):
         ("layout", C.c_int32),
         ("tile", C.c_int32),
         ("block", C.c_int32),
-        ("reserved", C.c_int32),
+        ("flags", C.c_int32),
     ]
 
 
@@ -276,9 +277,9 @@ class Result:
 
 def make_config(max_iter: int, required: int, tol: float, mode: str = "fast",
                 gradient: str = "adjoint", layout: int = LAYOUT_AUTO, tile: int = 0,
-                block: int = 0) -> BfgsConfig:
+                block: int = 0, flags: int = 0) -> BfgsConfig:
     return BfgsConfig(max_iter, required, tol, _MODES[mode], _GRADS[gradient],
-                      layout, tile, block, 0)
+                      layout, tile, block, flags)
 
 
 def Zeus(f: Objective, lower: float, upper: float, N: int, MAX_ITER: int,

@@ -29,7 +29,7 @@ namespace zb {
 
   struct ExactShared {
     double best, f1, fnew, ddir, sy, gnorm;
-    int accepted, done, status, stop;
+    int accepted, done, status, stop, executed;
   };
 
   template <class F, int D>
@@ -224,6 +224,7 @@ namespace zb {
             H[e] = sum + rho * s[i] * s[j];
           }
         }
+        const bool skipped = ::fabs(sh.sy) < kMinCurvature;
         __syncthreads();
         const bool take = sh.fnew < sh.best;
         if (take)
@@ -248,15 +249,25 @@ namespace zb {
             sh.status = kConverged;
             sh.fnew = sh.best;
             sh.done = 1;
+          } else if (!Traj && !take && skipped &&
+                     !(prm.flags & kFlagNoFixedPoint)) {
+            sh.done = 2; // fixed point: the rest would repeat this iteration
           }
           if constexpr (Traj)
             if (sh.done)
               out.traj_status[(size_t)iter * N + idx] = (int8_t)sh.status;
         }
         __syncthreads();
+        if (sh.done == 2) {
+          sh.executed = iter + 1;
+          iter = prm.max_iter;
+          break;
+        }
         if (sh.done)
           break;
       }
+      if (sh.done != 2)
+        sh.executed = iter;
       if (tid == 0) {
         if (sh.status == kUnset) { // bfgs_common.cuh:213-238
           sh.status = kSurrender;
@@ -278,7 +289,7 @@ namespace zb {
         if (out.gnorm)
           out.gnorm[idx] = sh.gnorm;
         if (out.counters) {
-          out.counters[3 * (size_t)idx + 0] = iter;
+          out.counters[3 * (size_t)idx + 0] = sh.executed;
           out.counters[3 * (size_t)idx + 1] = n_eval;
           out.counters[3 * (size_t)idx + 2] = n_grad;
         }

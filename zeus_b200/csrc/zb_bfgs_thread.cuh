@@ -93,7 +93,7 @@ namespace zb {
     for (int i = 0; i < D; ++i)
       p[i] = -g[i];
 
-    int status = kUnset, iter;
+    int status = kUnset, iter, executed = -1;
     double fout = best, gout = 0.0;
     for (iter = 0; iter < prm.max_iter; ++iter) {
       if (load_stop(ctl)) {
@@ -136,7 +136,8 @@ namespace zb {
         y[i] = gn[i] - g[i];
         sy = fma(s[i], y[i], sy);
       }
-      if (!(fabs(sy) < kMinCurvature)) {
+      const bool skipped = fabs(sy) < kMinCurvature;
+      if (!skipped) {
         const double rho = 1.0 / sy;
         double u[D], yu = 0.0;
 #pragma unroll
@@ -159,7 +160,8 @@ namespace zb {
           for (int j = i; j < D; ++j)
             H[tri<D>(i, j)] += s[i] * w[j] + w[i] * s[j];
       }
-      if (fnew < best) {
+      const bool take = fnew < best;
+      if (take) {
         best = fnew;
 #pragma unroll
         for (int i = 0; i < D; ++i) {
@@ -183,6 +185,11 @@ namespace zb {
         status = kConverged;
         fout = best;
         gout = gnrm;
+        break;
+      }
+      if (!take && skipped && !(prm.flags & kFlagNoFixedPoint)) {
+        executed = iter + 1; // fixed point: the rest would repeat this
+        iter = prm.max_iter;
         break;
       }
 #pragma unroll
@@ -217,7 +224,7 @@ namespace zb {
       for (int i = 0; i < D; ++i)
         out.x[idx * D + i] = x[i];
     if (out.counters) {
-      out.counters[3 * idx + 0] = iter;
+      out.counters[3 * idx + 0] = executed >= 0 ? executed : iter;
       out.counters[3 * idx + 1] = n_eval;
       out.counters[3 * idx + 2] = n_grad;
     }

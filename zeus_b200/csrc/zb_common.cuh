@@ -31,7 +31,10 @@ namespace zb {
     int max_iter;
     int required;
     double tol;
+    int flags; // ZEUS_FLAG_* (include/zeus_b200.h)
   };
+
+  inline constexpr int kFlagNoFixedPoint = 1;
 
   // Device view of zeus_run_outputs (include/zeus_b200.h).
   struct RunOut {

@@ -443,7 +443,7 @@ zeus_bfgs_device(const zeus_problem* problem, const zeus_bfgs_config* config,
   const size_t kws = need - nll_bytes(problem);
   Objective o = to_objective(problem, bins);
   BfgsParams prm{n, config->max_iter, config->required_converged,
-                 config->tolerance};
+                 config->tolerance, config->flags};
   RunOut ro{out->fval,     out->status, out->iter,   out->gnorm,
             out->x,        out->counters, out->traj_x, out->traj_f,
             out->traj_g,   out->traj_status};

@@ -11,8 +11,8 @@ from typing import Optional
 import numpy as np
 import torch
 
-from . import (BfgsConfig, CCensus, Objective, RunOutputs, check, lib,
-               make_config, LAYOUT_AUTO)
+from . import (BfgsConfig, Objective, RunOutputs, check, lib, make_config,
+               LAYOUT_AUTO)
 
 
 def _stream_handle(stream: Optional[torch.cuda.Stream]) -> int:
@@ -121,12 +121,12 @@ def bfgs_device(obj, starts: torch.Tensor, max_iter: int = 10000,
                 required: Optional[int] = None, tol: float = 1e-8,
                 mode: str = "fast", gradient: str = "adjoint",
                 layout: int = LAYOUT_AUTO, tile: int = 0, block: int = 0,
-                traj: bool = False, stream=None) -> BfgsRun:
+                traj: bool = False, stream=None, flags: int = 0) -> BfgsRun:
     """One BFGS per row of ``starts``; returns the BfgsRun with its outputs."""
     n = starts.shape[0]
     if required is None:
         required = n + 1  # stop-early off
-    cfg = make_config(max_iter, required, tol, mode, gradient, layout, tile, block)
+    cfg = make_config(max_iter, required, tol, mode, gradient, layout, tile, block, flags)
     r = BfgsRun(obj, n, cfg, device=starts.device, traj=traj)
     return r.launch(starts, stream=stream)
 
