@@ -37,6 +37,7 @@ def make_obj(kind, dim):
 
 
 def gpu_run(obj, starts, **kw):
+    """bfgs_device through the C ABI; host numpy results."""
     st = torch.from_numpy(np.ascontiguousarray(starts)).cuda()
     r = bfgs_device(obj, st, **kw)
     torch.cuda.synchronize()
@@ -240,3 +241,84 @@ def test_fast_mode_fixed_point_matches_full_iteration(cuda):
     for key in ("status", "iter", "fval", "gnorm", "x"):
         np.testing.assert_array_equal(a[key], b[key], err_msg=key)
     assert a["counters"][:, 0].sum() < b["counters"][:, 0].sum()
+
+
+# ---- tile and CTA layouts ----------------------------------------------------
+def _check_final(got, want, min_agree=0.9, dx_tol=1e-5):
+    agree = got["status"] == want["status"]
+    assert agree.mean() >= min_agree, f"status agreement {agree.mean():.2%}"
+    both = (got["status"] == 1) & (want["status"] == 1)
+    if both.sum() == 0:
+        return
+    df = np.abs(got["fval"][both] - want["fval"][both])
+    assert (df <= 1e-8 + 1e-10 * np.abs(want["fval"][both])).all(), df.max()
+    dx = np.abs(got["x"][both] - want["x"][both]).max()
+    assert dx <= dx_tol, dx
+
+
+@pytest.mark.parametrize("kind,dim,tile,n", [
+    (ROS, 8, 2, 96), (ROS, 8, 4, 96), (ROS, 8, 8, 96), (ROS, 16, 8, 48), (ROS, 32, 32, 16),
+    (ROS, 32, 16, 16), (RAS, 10, 4, 64), (RAS, 10, 16, 64), (ACK, 30, 32, 32),
+    (GAU, 32, 32, 16), (GAU, 8, 8, 32), (ROS, 4, 2, 64), (ROS, 2, 2, 128),
+])
+@pytest.mark.parametrize("grad", ["adjoint", "dual"])
+def test_tile_layout_final_results(cuda, kind, dim, tile, n, grad):
+    obj, data, idata = make_obj(kind, dim)
+    lo, hi = BOUNDS[kind]
+    st = O.oracle_starts(21, n, dim, lo, hi)
+    want = O.oracle_bfgs(kind, dim, st, max_iter=2000, data=data, idata=idata, lower=lo,
+                         upper=hi)
+    got = gpu_run(obj, st, max_iter=2000, mode="fast", gradient=grad,
+                  layout=zb.LAYOUT_TILE, tile=tile)
+    _check_final(got, want)
+
+
+def test_tile_layout_nll(cuda):
+    obj, x, k = make_obj(NLL, 4)
+    rng = np.random.default_rng(2)
+    lam = (1 - x) ** 10 / x ** (5 + 0.1 * np.log(x))
+    a0 = k.sum() / lam.sum()
+    st = np.column_stack([a0 * rng.uniform(0.8, 1.2, 32), rng.uniform(9, 11, 32),
+                          rng.uniform(4.5, 5.5, 32), rng.uniform(0.08, 0.12, 32)])
+    want = O.oracle_bfgs(NLL, 4, st, max_iter=3000, data=x, idata=k, lower=0, upper=10)
+    for tile in (2, 4, 8):
+        for grad in ("adjoint", "dual"):
+            got = gpu_run(obj, st, max_iter=3000, mode="fast", gradient=grad,
+                          layout=zb.LAYOUT_TILE, tile=tile)
+            fin = np.isfinite(want["fval"]) & np.isfinite(got["fval"])
+            np.testing.assert_allclose(got["fval"][fin], want["fval"][fin], rtol=1e-9)
+
+
+@pytest.mark.parametrize("kind,dim,n", [(ROS, 64, 8), (ROS, 128, 2), (GAU, 150, 2)])
+@pytest.mark.parametrize("grad", ["adjoint", "dual"])
+def test_cta_layout_final_results(cuda, kind, dim, n, grad):
+    obj, data, idata = make_obj(kind, dim)
+    lo, hi = BOUNDS[kind]
+    st = O.oracle_starts(13, n, dim, lo, hi)
+    iters = 600 if dim == 128 else 1500
+    want = O.oracle_bfgs(kind, dim, st, max_iter=iters, data=data, idata=idata, lower=lo,
+                         upper=hi)
+    got = gpu_run(obj, st, max_iter=iters, mode="fast", gradient=grad,
+                  layout=zb.LAYOUT_CTA)
+    _check_final(got, want, min_agree=0.5 if dim == 128 else 0.9, dx_tol=1e-4)
+    if kind == GAU:
+        assert (got["status"] == 1).all()
+        assert np.abs(got["x"]).max() < 1e-9
+
+
+@pytest.mark.parametrize("kind,dim", [(ROS, 2), (ROS, 4), (ROS, 8), (ROS, 10), (ROS, 16),
+                                      (ROS, 32), (ROS, 64), (ROS, 128), (RAS, 2), (RAS, 10),
+                                      (RAS, 16), (ACK, 2), (ACK, 10), (ACK, 30), (GAU, 2),
+                                      (GAU, 8), (GAU, 32), (GAU, 150)])
+def test_auto_layout_runs_everywhere(cuda, kind, dim):
+    obj, data, idata = make_obj(kind, dim)
+    lo, hi = BOUNDS[kind]
+    st = O.oracle_starts(5, 40, dim, lo, hi)
+    for grad in ("adjoint", "dual"):
+        got = gpu_run(obj, st, max_iter=50, mode="fast", gradient=grad)
+        assert set(np.unique(got["status"])) <= {0, 1, 5}
+        assert np.isfinite(got["fval"]).all()
+        # f(x_out) is the reported fval
+        for i in range(0, 40, 13):
+            assert got["fval"][i] == pytest.approx(O.value(kind, dim, got["x"][i], data),
+                                                   rel=1e-12, abs=1e-12)

@@ -38,6 +38,9 @@ COMMON = [
 UNITS = [
     ("zb_exact.cu", ["-fmad=false"]),
     ("zb_fast.cu", []),
+    ("zb_fast_thread.cu", []),
+    ("zb_fast_tile.cu", []),
+    ("zb_fast_cta.cu", []),
     ("zb_runtime.cu", []),
 ]
 

@@ -1,0 +1,549 @@
+// Fast BFGS with one optimisation per cooperating group:
+//
+//   bfgs_tile_kernel  (mid D, up to 32): a tile of TS lanes per run.  Lane l
+//     owns coordinates l, l+TS, ... (R = ceil(D/TS) of them) and the same rows
+//     of the inverse Hessian H, in registers.  Vectors other lanes need (y, s,
+//     w, g for H products; the trial point for f) go through a small
+//     per-tile shared buffer; scalars through butterfly shuffles.
+//
+//   bfgs_cta_kernel   (large D, up to ~160): a thread block per run, H in
+//     shared memory (D x D doubles, kept exactly symmetric).  One sweep
+//     reads H once and forms both u = H y and h = H g_next (thread t walks
+//     column t % D over a 1/Q share of the rows; Q = blockDim / D partial
+//     sums meet in shared memory) -- column walks by consecutive threads are
+//     bank-conflict free; a second sweep applies the rank-2 update in place.
+//     The next search direction follows without a third sweep:
+//     H+ g = h + s (w.g) + w (s.g).
+//
+// Both keep the reference's iteration semantics (line search, skip rule,
+// accept-if-better, status protocol) and the fixed-point exit.  The update
+// H+ = H + s w^T + w s^T forms each product with __dmul_rn so that entry
+// (i, j) and (j, i) round identically and H stays exactly symmetric (the
+// CTA kernel reads columns as rows).
+#pragma once
+
+#include "zb_bfgs_thread.cuh"
+#include "zb_common.cuh"
+#include "zb_group.cuh"
+
+namespace zb {
+
+  template <class F, class G>
+  concept HasValueCoop = requires(const F& f, const G& g, const double* x) {
+    { f.value_coop(g, x) } -> std::convertible_to<double>;
+  };
+  template <class F, class G>
+  concept HasAdjointCoop =
+    requires(const F& f, const G& g, const double* x, double* gr) {
+      { f.adjoint_coop(g, x, gr) } -> std::convertible_to<double>;
+    };
+  template <class F>
+  concept TrialsWithGradient = requires { F::kTrialsWithGradient; };
+
+  // f(x) for a shared x, the same value in every member.
+  template <class F, int D, class G>
+  __device__ __forceinline__ double
+  coop_value(const F& f, const G& grp, const double* x)
+  {
+    if constexpr (HasValueCoop<F, G>) {
+      return f.value_coop(grp, x);
+    } else {
+      double v = 0.0;
+      if (grp.rank() == 0)
+        v = fast_value<F, D>(f, x);
+      return grp.bcast(v, 0);
+    }
+  }
+
+  // g = grad f(x) into shared g (one member per entry); the caller syncs
+  // before reading it.  Returns f(x) when the adjoint computed it, else NaN.
+  template <class F, int D, bool Adjoint, class G>
+  __device__ __forceinline__ double
+  coop_gradient(const F& f, const G& grp, const double* x, double* g)
+  {
+    if constexpr (Adjoint && HasAdjointCoop<F, G>) {
+      return f.adjoint_coop(grp, x, g);
+    } else if constexpr (Adjoint && HasAdjoint<F>) {
+      double v = 0.0;
+      if (grp.rank() == 0)
+        v = f.adjoint(x, g);
+      return grp.bcast(v, 0);
+    } else {
+      // the plain form: D forward dual passes spread over the members
+      for (int i = grp.rank(); i < D; i += grp.size()) {
+        std::array<dual::DualNumber, D> xd;
+#pragma unroll 1
+        for (int j = 0; j < D; ++j)
+          xd[j] = dual::DualNumber(x[j], 0.0);
+        xd[i].dual = 1.0;
+        g[i] = f(xd).dual;
+      }
+      return __longlong_as_double(0x7ff8000000000000ll);
+    }
+  }
+
+  // ---------------------------------------------------------------- tile
+  inline constexpr int kTileBlock = 128;
+
+  template <int D, int TS>
+  constexpr int
+  tile_smem_doubles()
+  {
+    return 4 * D + TS; // xs, gs, b1, b2, scratch
+  }
+
+  template <class F, int D, int TS, bool Adjoint>
+  __global__ void __launch_bounds__(kTileBlock)
+    bfgs_tile_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
+                     RunOut out, Control* ctl)
+  {
+    constexpr int R = (D + TS - 1) / TS;
+    constexpr int TPB = kTileBlock / TS;
+    extern __shared__ double sm[];
+    auto tile = cg::tiled_partition<TS>(cg::this_thread_block());
+    const int tslot = threadIdx.x / TS;
+    const int lane = (int)tile.thread_rank();
+    double* xs = sm + tslot * tile_smem_doubles<D, TS>();
+    double* gs = xs + D;
+    double* b1 = gs + D;
+    double* b2 = b1 + D;
+    TileGroup<TS> grp(tile, b2 + D);
+    const int64_t run = (int64_t)blockIdx.x * TPB + tslot;
+    if (run >= prm.n)
+      return; // the whole tile leaves together
+
+    double x[R], g[R], p[R], H[R][D];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = lane + r * TS;
+      x[r] = i < D ? starts[run * D + i] : 0.0;
+      if (i < D)
+        xs[i] = x[r];
+#pragma unroll
+      for (int j = 0; j < D; ++j)
+        H[r][j] = (i == j) ? 1.0 : 0.0;
+    }
+    grp.sync();
+    double best = coop_value<F, D>(f, grp, xs);
+    coop_gradient<F, D, Adjoint>(f, grp, xs, gs);
+    grp.sync();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = lane + r * TS;
+      g[r] = i < D ? gs[i] : 0.0;
+      p[r] = -g[r];
+    }
+    long long n_eval = 1, n_grad = 1;
+    int status = kUnset, iter, executed = -1;
+    double fout = best, gout = 0.0;
+
+    for (iter = 0; iter < prm.max_iter; ++iter) {
+      const int stop = grp.bcast(lane == 0 ? load_stop(ctl) : 0, 0);
+      if (stop) {
+        status = kStopped;
+        break;
+      }
+      double dd = 0.0;
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        dd = fma(g[r], p[r], dd);
+      const double ddir = grp.sum(dd);
+      double xn[R], alpha = 1.0, fnew = 0.0;
+      bool ok = false;
+      for (int k = 0; k <= kLineSearchTrials; ++k) {
+        grp.sync(); // earlier readers of xs are done
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int i = lane + r * TS;
+          xn[r] = fma(alpha, p[r], x[r]);
+          if (i < D)
+            xs[i] = xn[r];
+        }
+        grp.sync();
+        const double f1 = coop_value<F, D>(f, grp, xs);
+        ++n_eval;
+        if (k == kLineSearchTrials) { // all 20 failed: alpha = 2^-20
+          fnew = f1;
+          break;
+        }
+        if (f1 <= best + kArmijoC1 * alpha * ddir && f1 < best) {
+          ok = true;
+          fnew = f1;
+          break;
+        }
+        alpha *= 0.5;
+      }
+      (void)ok;
+      grp.sync();
+      coop_gradient<F, D, Adjoint>(f, grp, xs, gs);
+      ++n_grad;
+      grp.sync();
+      double gn[R], s[R], y[R];
+      double sy_part = 0.0;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = lane + r * TS;
+        gn[r] = i < D ? gs[i] : 0.0;
+        s[r] = xn[r] - x[r];
+        y[r] = gn[r] - g[r];
+        sy_part = fma(s[r], y[r], sy_part);
+      }
+      const double sy = grp.sum(sy_part);
+      const bool skipped = fabs(sy) < kMinCurvature;
+      if (!skipped) {
+        const double rho = 1.0 / sy;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int i = lane + r * TS;
+          if (i < D)
+            b1[i] = y[r];
+        }
+        grp.sync();
+        double u[R], yu_part = 0.0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          double a = 0.0;
+#pragma unroll
+          for (int j = 0; j < D; ++j)
+            a = fma(H[r][j], b1[j], a);
+          u[r] = a;
+          yu_part = fma(y[r], a, yu_part);
+        }
+        const double yu = grp.sum(yu_part);
+        const double hb = 0.5 * rho * fma(rho, yu, 1.0);
+        double w[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          w[r] = fma(hb, s[r], -rho * u[r]);
+        grp.sync(); // b1 (= y) fully read
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int i = lane + r * TS;
+          if (i < D) {
+            b1[i] = s[r];
+            b2[i] = w[r];
+          }
+        }
+        grp.sync();
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+          for (int j = 0; j < D; ++j)
+            H[r][j] += __dadd_rn(__dmul_rn(s[r], b2[j]), __dmul_rn(w[r], b1[j]));
+      }
+      const bool take = fnew < best;
+      if (take) {
+        best = fnew;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          x[r] = xn[r];
+          g[r] = gn[r];
+        }
+      }
+      double gg = 0.0;
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        gg = fma(g[r], g[r], gg);
+      const double gnrm = sqrt(grp.sum(gg));
+      if (!isfinite(gnrm) || !isfinite(fnew)) {
+        status = kNonFinite;
+        fout = fnew;
+        gout = gnrm;
+        break;
+      }
+      if (gnrm < prm.tol) {
+        if (lane == 0)
+          note_converged(ctl, prm.required);
+        status = kConverged;
+        fout = best;
+        gout = gnrm;
+        break;
+      }
+      if (!take && skipped && !(prm.flags & kFlagNoFixedPoint)) {
+        executed = iter + 1;
+        iter = prm.max_iter;
+        break;
+      }
+      grp.sync(); // b1 / b2 fully read
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = lane + r * TS;
+        if (i < D)
+          b1[i] = g[r];
+      }
+      grp.sync();
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        double a = 0.0;
+#pragma unroll
+        for (int j = 0; j < D; ++j)
+          a = fma(H[r][j], b1[j], a);
+        p[r] = -a;
+      }
+    }
+    if (status == kUnset || status == kStopped) {
+      if (status == kUnset)
+        status = kSurrender;
+      fout = best;
+      double gg = 0.0;
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        gg = fma(g[r], g[r], gg);
+      gout = sqrt(grp.sum(gg));
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = lane + r * TS;
+      if (out.x && i < D)
+        out.x[run * D + i] = x[r];
+    }
+    if (lane == 0) {
+      if (out.fval)
+        out.fval[run] = fout;
+      if (out.status)
+        out.status[run] = status;
+      if (out.iter)
+        out.iter[run] = iter;
+      if (out.gnorm)
+        out.gnorm[run] = gout;
+      if (out.counters) {
+        out.counters[3 * run + 0] = executed >= 0 ? executed : iter;
+        out.counters[3 * run + 1] = n_eval;
+        out.counters[3 * run + 2] = n_grad;
+      }
+    }
+  }
+
+  // ---------------------------------------------------------------- CTA
+  // Shared-memory layout (doubles): H[D*D] | 11 vectors of D | partial sums
+  // 2*Q*D | reduction 32*8 | scratch blockDim | flags (as doubles) 4.
+  template <int D>
+  __host__ __device__ constexpr size_t
+  cta_smem_doubles(int block)
+  {
+    const int q = block >= D ? block / D : 1;
+    return (size_t)D * D + 11 * D + 2 * q * D + 32 * 8 + block + 4;
+  }
+
+  template <class F, int D, bool Adjoint, int kBlock>
+  __global__ void __launch_bounds__(kBlock)
+    bfgs_cta_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
+                    RunOut out, Control* ctl)
+  {
+    constexpr int Q = kBlock >= D ? kBlock / D : 1;
+    extern __shared__ double sm[];
+    double* H = sm;
+    double* x = H + D * D;
+    double* g = x + D;
+    double* p = g + D;
+    double* xn = p + D;
+    double* gn = xn + D;
+    double* s = gn + D;
+    double* y = s + D;
+    double* w = y + D;
+    double* u = w + D;
+    double* h = u + D;
+    double* gt = h + D; // gradient computed at line-search trials
+    double* partU = gt + D;
+    double* partH = partU + Q * D;
+    double* red = partH + Q * D;
+    double* scratch = red + 32 * 8;
+    int* flags = reinterpret_cast<int*>(scratch + kBlock);
+    CtaGroup grp{red, scratch};
+    const int t = threadIdx.x;
+    constexpr bool kTrialGrad = Adjoint && TrialsWithGradient<F>;
+
+    for (int64_t run = blockIdx.x; run < prm.n; run += gridDim.x) {
+      for (int i = t; i < D; i += kBlock)
+        x[i] = starts[run * D + i];
+      for (int e = t; e < D * D; e += kBlock)
+        H[e] = (e / D == e % D) ? 1.0 : 0.0;
+      __syncthreads();
+      double best;
+      if constexpr (kTrialGrad)
+        best = coop_gradient<F, D, Adjoint>(f, grp, x, g);
+      else {
+        best = coop_value<F, D>(f, grp, x);
+        coop_gradient<F, D, Adjoint>(f, grp, x, g);
+      }
+      __syncthreads();
+      for (int i = t; i < D; i += kBlock)
+        p[i] = -g[i];
+      long long n_eval = 1, n_grad = 1;
+      int status = kUnset, iter, executed = -1;
+      double fout = best, gout = 0.0;
+      __syncthreads();
+
+      for (iter = 0; iter < prm.max_iter; ++iter) {
+        if (t == 0)
+          flags[0] = load_stop(ctl);
+        __syncthreads();
+        if (flags[0]) {
+          status = kStopped;
+          break;
+        }
+        double dd = 0.0;
+        for (int i = t; i < D; i += kBlock)
+          dd = fma(g[i], p[i], dd);
+        const double ddir = grp.sum(dd);
+        double alpha = 1.0, fnew = 0.0;
+        bool have_grad = false;
+        for (int k = 0; k <= kLineSearchTrials; ++k) {
+          for (int i = t; i < D; i += kBlock)
+            xn[i] = fma(alpha, p[i], x[i]);
+          __syncthreads();
+          double f1;
+          if constexpr (kTrialGrad)
+            f1 = coop_gradient<F, D, Adjoint>(f, grp, xn, gt);
+          else
+            f1 = coop_value<F, D>(f, grp, xn);
+          ++n_eval;
+          if (k == kLineSearchTrials) {
+            fnew = f1;
+            have_grad = kTrialGrad;
+            break;
+          }
+          if (f1 <= best + kArmijoC1 * alpha * ddir && f1 < best) {
+            fnew = f1;
+            have_grad = kTrialGrad;
+            break;
+          }
+          alpha *= 0.5;
+          __syncthreads(); // xn fully read before the next trial writes it
+        }
+        __syncthreads();
+        if (have_grad) {
+          for (int i = t; i < D; i += kBlock)
+            gn[i] = gt[i];
+        } else {
+          coop_gradient<F, D, Adjoint>(f, grp, xn, gn);
+          ++n_grad;
+        }
+        __syncthreads();
+        if (have_grad)
+          ++n_grad;
+        const bool take = fnew < best;
+        double sy_part = 0.0;
+        for (int i = t; i < D; i += kBlock) {
+          s[i] = xn[i] - x[i];
+          y[i] = gn[i] - g[i];
+          sy_part = fma(s[i], y[i], sy_part);
+        }
+        const double sy = grp.sum(sy_part); // (its barriers publish s, y)
+        const bool skipped = fabs(sy) < kMinCurvature;
+        const double* gnext = take ? gn : g;
+        // sweep 1: u = H y (if updating) and h = H g_next, by columns
+        {
+          const int i = t % D, q = t / D;
+          if (q < Q && t < Q * D) {
+            double au = 0.0, ah = 0.0;
+            for (int m = q; m < D; m += Q) {
+              const double hv = H[m * D + i];
+              ah = fma(hv, gnext[m], ah);
+              if (!skipped)
+                au = fma(hv, y[m], au);
+            }
+            partU[q * D + i] = au;
+            partH[q * D + i] = ah;
+          }
+        }
+        __syncthreads();
+        double yu_part = 0.0;
+        for (int i = t; i < D; i += kBlock) {
+          double au = 0.0, ah = 0.0;
+          for (int q = 0; q < Q; ++q) {
+            au += partU[q * D + i];
+            ah += partH[q * D + i];
+          }
+          u[i] = au;
+          h[i] = ah;
+          yu_part = fma(y[i], au, yu_part);
+        }
+        if (!skipped) {
+          const double yu = grp.sum(yu_part);
+          const double rho = 1.0 / sy;
+          const double hb = 0.5 * rho * fma(rho, yu, 1.0);
+          double wg = 0.0, sg = 0.0;
+          for (int i = t; i < D; i += kBlock) {
+            const double wi = fma(hb, s[i], -rho * u[i]);
+            w[i] = wi;
+            wg = fma(wi, gnext[i], wg);
+            sg = fma(s[i], gnext[i], sg);
+          }
+          double v[2] = {wg, sg};
+          grp.template sum<2>(v); // barriers publish w
+          // sweep 2: H += s w^T + w s^T
+          for (int e = t; e < D * D; e += kBlock) {
+            const int i = e / D, j = e - (e / D) * D;
+            H[e] += __dadd_rn(__dmul_rn(s[i], w[j]), __dmul_rn(w[i], s[j]));
+          }
+          for (int i = t; i < D; i += kBlock)
+            p[i] = -(h[i] + s[i] * v[0] + w[i] * v[1]);
+        } else {
+          for (int i = t; i < D; i += kBlock)
+            p[i] = -h[i];
+        }
+        if (take) {
+          best = fnew;
+          for (int i = t; i < D; i += kBlock) {
+            x[i] = xn[i];
+            g[i] = gn[i];
+          }
+        }
+        __syncthreads();
+        double gg = 0.0;
+        for (int i = t; i < D; i += kBlock)
+          gg = fma(g[i], g[i], gg);
+        const double gnrm = sqrt(grp.sum(gg));
+        if (!isfinite(gnrm) || !isfinite(fnew)) {
+          status = kNonFinite;
+          fout = fnew;
+          gout = gnrm;
+          break;
+        }
+        if (gnrm < prm.tol) {
+          if (t == 0)
+            note_converged(ctl, prm.required);
+          status = kConverged;
+          fout = best;
+          gout = gnrm;
+          break;
+        }
+        if (!take && skipped && !(prm.flags & kFlagNoFixedPoint)) {
+          executed = iter + 1;
+          iter = prm.max_iter;
+          break;
+        }
+      }
+      if (status == kUnset || status == kStopped) {
+        if (status == kUnset)
+          status = kSurrender;
+        fout = best;
+        double gg = 0.0;
+        for (int i = t; i < D; i += kBlock)
+          gg = fma(g[i], g[i], gg);
+        gout = sqrt(grp.sum(gg));
+      }
+      if (out.x)
+        for (int i = t; i < D; i += kBlock)
+          out.x[run * D + i] = x[i];
+      if (t == 0) {
+        if (out.fval)
+          out.fval[run] = fout;
+        if (out.status)
+          out.status[run] = status;
+        if (out.iter)
+          out.iter[run] = iter;
+        if (out.gnorm)
+          out.gnorm[run] = gout;
+        if (out.counters) {
+          out.counters[3 * run + 0] = executed >= 0 ? executed : iter;
+          out.counters[3 * run + 1] = n_eval;
+          out.counters[3 * run + 2] = n_grad;
+        }
+      }
+      __syncthreads();
+    }
+  }
+
+} // namespace zb

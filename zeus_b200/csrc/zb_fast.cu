@@ -1,19 +1,46 @@
-// Fast-mode BFGS launchers: layout chosen by dimension.
-#include "zb_bfgs_thread.cuh"
+// Fast-mode dispatcher: picks the layout for (objective, dimension) unless
+// the configuration names one (the autotuner sweeps them that way).
 #include "zb_objective_visit.cuh"
 
 namespace zb {
 
-  namespace {
-    constexpr int kThreadBlock = 128;
-    constexpr int kMaxThreadDim = 10; // H (55 doubles) + vectors in registers
-  } // namespace
+  void
+  default_layout(int kind, int dim, int* layout, int* tile)
+  {
+    *tile = 0;
+    if (dim <= 4 && thread_layout_supported(kind, dim)) {
+      *layout = ZEUS_LAYOUT_THREAD;
+      return;
+    }
+    const unsigned w = tile_widths(kind, dim);
+    if (w) {
+      // narrowest tile whose rows of H fit in about 40 doubles per lane
+      for (int k = 1; k <= 5; ++k) {
+        const int ts = 1 << k;
+        const int r = (dim + ts - 1) / ts;
+        if ((w >> k) & 1u) {
+          *tile = ts;
+          if (r * dim <= 40)
+            break;
+        }
+      }
+      *layout = ZEUS_LAYOUT_TILE;
+      return;
+    }
+    if (cta_layout_supported(kind, dim)) {
+      *layout = ZEUS_LAYOUT_CTA;
+      return;
+    }
+    *layout = thread_layout_supported(kind, dim) ? ZEUS_LAYOUT_THREAD : -1;
+  }
 
   bool
   fast_supported(int kind, int dim, int gradient)
   {
     (void)gradient;
-    return builtin_supported(kind, dim) && dim <= kMaxThreadDim;
+    return builtin_supported(kind, dim) &&
+           (thread_layout_supported(kind, dim) || tile_widths(kind, dim) != 0 ||
+            cta_layout_supported(kind, dim));
   }
 
   size_t
@@ -35,25 +62,37 @@ namespace zb {
     (void)ws_bytes;
     if (prm.n <= 0)
       return ZEUS_OK;
-    const bool adjoint = c.gradient == ZEUS_GRAD_ADJOINT;
-    return visit_objective(o, [&](auto f) -> int {
-      using F = decltype(f);
-      constexpr int D = (int)F::arity;
-      if constexpr (D <= kMaxThreadDim) {
-        const int block = c.block > 0 ? c.block : kThreadBlock;
-        const unsigned grid = (unsigned)((prm.n + block - 1) / block);
-        if (adjoint)
-          bfgs_thread_kernel<F, D, true>
-            <<<grid, block, 0, st>>>(f, prm, starts, out, ctl);
-        else
-          bfgs_thread_kernel<F, D, false>
-            <<<grid, block, 0, st>>>(f, prm, starts, out, ctl);
-        return cuda_fail(cudaGetLastError(), "fast BFGS launch");
-      } else {
-        set_error("fast BFGS: dim %d has no layout built", D);
-        return ZEUS_E_UNSUPPORTED;
+    int layout = c.layout, tile = c.tile;
+    if (layout == ZEUS_LAYOUT_AUTO)
+      default_layout(o.kind, o.dim, &layout, &tile);
+    switch (layout) {
+      case ZEUS_LAYOUT_THREAD:
+        if (!thread_layout_supported(o.kind, o.dim))
+          break;
+        return launch_thread(o, c, prm, starts, out, ctl, st);
+      case ZEUS_LAYOUT_TILE: {
+        const unsigned w = tile_widths(o.kind, o.dim);
+        if (tile == 0) {
+          int l2;
+          default_layout(o.kind, o.dim, &l2, &tile);
+          if (l2 != ZEUS_LAYOUT_TILE)
+            tile = 0;
+        }
+        if (tile < 2 || tile > 32 || (tile & (tile - 1)) ||
+            !((w >> __builtin_ctz((unsigned)tile)) & 1u))
+          break;
+        return launch_tile(o, c, tile, prm, starts, out, ctl, st);
       }
-    });
+      case ZEUS_LAYOUT_CTA:
+        if (!cta_layout_supported(o.kind, o.dim))
+          break;
+        return launch_cta(o, c, prm, starts, out, ctl, st);
+      default:
+        break;
+    }
+    set_error("fast BFGS: layout %d (tile %d) is not built for kind %d dim %d",
+              layout, tile, o.kind, o.dim);
+    return ZEUS_E_UNSUPPORTED;
   }
 
 } // namespace zb

@@ -1,0 +1,83 @@
+// CTA-per-run fast BFGS launcher (D > 32, H in shared memory).
+#include "zb_bfgs_coop.cuh"
+#include "zb_objective_visit.cuh"
+
+namespace zb {
+
+  namespace {
+    constexpr int kMinCtaDim = 33;
+    constexpr size_t kSmemLimit = 227 * 1024;
+
+    template <int D>
+    constexpr int
+    cta_block()
+    {
+      return D <= 64 ? 256 : 512;
+    }
+
+    template <class F, int D, bool Adj>
+    int
+    launch_one(const F& f, const BfgsParams& prm, const double* starts,
+               const RunOut& out, Control* ctl, cudaStream_t st)
+    {
+      constexpr int B = cta_block<D>();
+      const size_t smem = sizeof(double) * cta_smem_doubles<D>(B);
+      auto kern = bfgs_cta_kernel<F, D, Adj, B>;
+      int rc = cuda_fail(cudaFuncSetAttribute(
+                           kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem),
+                         "CTA-layout shared memory attribute");
+      if (rc)
+        return rc;
+      int per_sm = 0;
+      rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                       &per_sm, kern, B, smem),
+                     "CTA-layout occupancy");
+      if (rc)
+        return rc;
+      if (per_sm < 1) {
+        set_error("CTA layout: dim %d does not fit on an SM", D);
+        return ZEUS_E_UNSUPPORTED;
+      }
+      const int64_t cap = (int64_t)sm_count() * per_sm;
+      const unsigned grid = (unsigned)(prm.n < cap ? prm.n : cap);
+      kern<<<grid, B, smem, st>>>(f, prm, starts, out, ctl);
+      return cuda_fail(cudaGetLastError(), "CTA-layout BFGS launch");
+    }
+  } // namespace
+
+  bool
+  cta_layout_supported(int kind, int dim)
+  {
+    if (!builtin_supported(kind, dim) || dim < kMinCtaDim)
+      return false;
+    const int b = dim <= 64 ? 256 : 512;
+    const int q = b >= dim ? b / dim : 1;
+    const size_t d =
+      (size_t)dim * dim + 11 * dim + 2 * q * dim + 32 * 8 + b + 4;
+    return d * sizeof(double) <= kSmemLimit;
+  }
+
+  int
+  launch_cta(const Objective& o, const zeus_bfgs_config& c,
+             const BfgsParams& prm, const double* starts, const RunOut& out,
+             Control* ctl, cudaStream_t st)
+  {
+    const bool adjoint = c.gradient == ZEUS_GRAD_ADJOINT;
+    return visit_objective(o, [&](auto f) -> int {
+      using F = decltype(f);
+      constexpr int D = (int)F::arity;
+      if constexpr (D >= kMinCtaDim &&
+                    sizeof(double) * cta_smem_doubles<D>(cta_block<D>()) <=
+                      kSmemLimit) {
+        if (adjoint)
+          return launch_one<F, D, true>(f, prm, starts, out, ctl, st);
+        return launch_one<F, D, false>(f, prm, starts, out, ctl, st);
+      } else {
+        set_error("CTA layout: dim %d not built", D);
+        return ZEUS_E_UNSUPPORTED;
+      }
+    });
+  }
+
+} // namespace zb

@@ -43,7 +43,24 @@ namespace zb {
                  double* pbx, double* pbf, double* gbest, void* ws,
                  size_t ws_bytes, cudaStream_t st);
 
-  // fast mode (zb_fast.cu)
+  // fast-mode layouts (zb_fast_thread.cu, zb_fast_tile.cu, zb_fast_cta.cu)
+  bool thread_layout_supported(int kind, int dim);
+  int launch_thread(const Objective& o, const zeus_bfgs_config& c,
+                    const BfgsParams& prm, const double* starts,
+                    const RunOut& out, Control* ctl, cudaStream_t st);
+  // tile widths built for dim (bit k set: width 2^k available)
+  unsigned tile_widths(int kind, int dim);
+  int launch_tile(const Objective& o, const zeus_bfgs_config& c, int tile,
+                  const BfgsParams& prm, const double* starts,
+                  const RunOut& out, Control* ctl, cudaStream_t st);
+  bool cta_layout_supported(int kind, int dim);
+  int launch_cta(const Objective& o, const zeus_bfgs_config& c,
+                 const BfgsParams& prm, const double* starts,
+                 const RunOut& out, Control* ctl, cudaStream_t st);
+  // default layout / tile width for (kind, dim): ZEUS_LAYOUT_* and width
+  void default_layout(int kind, int dim, int* layout, int* tile);
+
+  // fast mode dispatcher (zb_fast.cu)
   bool fast_supported(int kind, int dim, int gradient);
   size_t fast_workspace_bytes(const Objective& o, const zeus_bfgs_config& c,
                               int64_t n);

@@ -84,6 +84,39 @@ namespace zeus {
       g[D - 1] = carry;
       return sum;
     }
+
+    // Cooperative forms: member k takes terms / coordinates k, k+size, ...
+    template <class G>
+    __device__ double
+    value_coop(const G& grp, const double* x) const
+    {
+      double part = 0.0;
+      for (int i = grp.rank(); i < (int)D - 1; i += grp.size()) {
+        const double t1 = 1.0 - x[i];
+        const double t2 = fma(-x[i], x[i], x[i + 1]);
+        part = fma(100.0 * t2, t2, fma(t1, t1, part));
+      }
+      return grp.sum(part);
+    }
+    template <class G>
+    __device__ double
+    adjoint_coop(const G& grp, const double* x, double* g) const
+    {
+      double part = 0.0;
+      for (int i = grp.rank(); i < (int)D; i += grp.size()) {
+        double gi = 0.0;
+        if (i + 1 < (int)D) {
+          const double t1 = 1.0 - x[i];
+          const double t2 = fma(-x[i], x[i], x[i + 1]);
+          part = fma(100.0 * t2, t2, fma(t1, t1, part));
+          gi = -2.0 * t1 - 400.0 * x[i] * t2;
+        }
+        if (i > 0)
+          gi = fma(200.0, fma(-x[i - 1], x[i - 1], x[i]), gi);
+        g[i] = gi;
+      }
+      return grp.sum(part);
+    }
   };
 
   template <std::size_t D>
@@ -130,6 +163,29 @@ namespace zeus {
         g[i] = fma(10.0 * kTwoPi, s, 2.0 * x[i]);
       }
       return sum;
+    }
+
+    template <class G>
+    __device__ double
+    value_coop(const G& grp, const double* x) const
+    {
+      double part = 0.0;
+      for (int i = grp.rank(); i < (int)D; i += grp.size())
+        part += fma(x[i], x[i], -10.0 * ::cospi(2.0 * x[i]));
+      return 10.0 * D + grp.sum(part);
+    }
+    template <class G>
+    __device__ double
+    adjoint_coop(const G& grp, const double* x, double* g) const
+    {
+      double part = 0.0;
+      for (int i = grp.rank(); i < (int)D; i += grp.size()) {
+        double s, c;
+        ::sincospi(2.0 * x[i], &s, &c);
+        part += fma(x[i], x[i], -10.0 * c);
+        g[i] = fma(10.0 * kTwoPi, s, 2.0 * x[i]);
+      }
+      return 10.0 * D + grp.sum(part);
     }
   };
 
@@ -198,6 +254,42 @@ namespace zeus {
         g[i] = fma(a, x[i], b * g[i]);
       return -20.0 * e1 - e2 + 20.0 + 2.718281828459045;
     }
+
+    template <class G>
+    __device__ double
+    value_coop(const G& grp, const double* x) const
+    {
+      double v[2] = {0.0, 0.0};
+      for (int i = grp.rank(); i < (int)D; i += grp.size()) {
+        v[0] = fma(x[i], x[i], v[0]);
+        v[1] += ::cospi(2.0 * x[i]);
+      }
+      grp.template sum<2>(v);
+      constexpr double inv = 1.0 / double(D);
+      return -20.0 * ::exp(-0.2 * ::sqrt(v[0] * inv)) - ::exp(v[1] * inv) + 20.0 +
+             2.718281828459045;
+    }
+    template <class G>
+    __device__ double
+    adjoint_coop(const G& grp, const double* x, double* g) const
+    {
+      double v[2] = {0.0, 0.0};
+      for (int i = grp.rank(); i < (int)D; i += grp.size()) {
+        double s, c;
+        ::sincospi(2.0 * x[i], &s, &c);
+        v[0] = fma(x[i], x[i], v[0]);
+        v[1] += c;
+        g[i] = s; // the same member finishes g[i] below
+      }
+      grp.template sum<2>(v);
+      constexpr double inv = 1.0 / double(D);
+      const double r = ::sqrt(v[0] * inv);
+      const double e1 = ::exp(-0.2 * r), e2 = ::exp(v[1] * inv);
+      const double a = 4.0 * e1 * inv / r, b = kTwoPi * e2 * inv;
+      for (int i = grp.rank(); i < (int)D; i += grp.size())
+        g[i] = fma(a, x[i], b * g[i]);
+      return -20.0 * e1 - e2 + 20.0 + 2.718281828459045;
+    }
   };
 
   // 0.5 x^T C x with C a dense D x D row-major device matrix.
@@ -255,6 +347,73 @@ namespace zeus {
       }
       return 0.5 * q;
     }
+
+    // r = C^T x, split over Q = size/D segments of j so that every member
+    // works; member t owns column i = t % D and segment t / D.  Reads of C
+    // are coalesced (consecutive members, consecutive i).  The partial sums
+    // meet in grp.scratch (size() doubles).  x^T C^T x = x^T C x, so f comes
+    // from C^T x even when C is not symmetric.
+    template <class G>
+    __device__ void
+    ctx_coop(const G& grp, const double* x, const double* M, double* r) const
+    {
+      const int t = grp.rank(), nq = grp.size() >= (int)D ? grp.size() / (int)D : 1;
+      if (nq == 1) {
+        grp.sync();
+        for (int i = t; i < (int)D; i += grp.size()) {
+          double a = 0.0;
+          for (int j = 0; j < (int)D; ++j)
+            a = fma(M[j * D + i], x[j], a);
+          r[i] = a;
+        }
+        grp.sync();
+        return;
+      }
+      const int i = t % (int)D, q = t / (int)D;
+      double a = 0.0;
+      if (q < nq)
+        for (int j = q; j < (int)D; j += nq)
+          a = fma(M[j * D + i], x[j], a);
+      grp.sync();
+      if (q < nq)
+        grp.scratch[q * D + i] = a;
+      grp.sync();
+      if (t < (int)D) {
+        double b = 0.0;
+        for (int k = 0; k < nq; ++k)
+          b += grp.scratch[k * D + t];
+        r[t] = b;
+      }
+      grp.sync();
+    }
+
+    // f = 0.5 x.(C^T x); g = C^T x (symmetric C) else (C x + C^T x) / 2.
+    // `g` must be shared by the group (it is written by one member per i
+    // and read back by all after the final sync).
+    template <class G>
+    __device__ double
+    adjoint_coop(const G& grp, const double* x, double* g) const
+    {
+      ctx_coop(grp, x, C, g);
+      double part = 0.0;
+      for (int i = grp.rank(); i < (int)D; i += grp.size())
+        part = fma(x[i], g[i], part);
+      const double f = 0.5 * grp.sum(part);
+      if (!symmetric) {
+        // C x = (C^T)^T x: same kernel on the transpose via row reads
+        for (int i = grp.rank(); i < (int)D; i += grp.size()) {
+          double a = 0.0;
+          for (int j = 0; j < (int)D; ++j)
+            a = fma(C[i * D + j], x[j], a);
+          g[i] = 0.5 * (g[i] + a);
+        }
+        grp.sync();
+      }
+      return f;
+    }
+    // The value costs the same matrix-vector product as the gradient; the
+    // kernels evaluate line-search trials with adjoint_coop and keep g.
+    static constexpr bool kTrialsWithGradient = true;
   };
 
   // Binned Poisson negative log-likelihood of the dijet shape
@@ -328,6 +487,49 @@ namespace zeus {
       g[2] = g2;
       g[3] = g3;
       return nll;
+    }
+
+    // Cooperative forms split the bins over the group.
+    template <class G>
+    __device__ double
+    value_coop(const G& grp, const double* th) const
+    {
+      const double la = ::log(th[0]);
+      double part = 0.0;
+      for (int i = grp.rank(); i < nbins; i += grp.size()) {
+        const double lx = bins[4 * i], l1 = bins[4 * i + 1];
+        const double k = bins[4 * i + 2], lgk = bins[4 * i + 3];
+        const double ll = la + fma(th[1], l1, -fma(th[3], lx, th[2]) * lx);
+        part += ::exp(ll) - fma(k, ll, -lgk);
+      }
+      return grp.sum(part);
+    }
+    template <class G>
+    __device__ double
+    adjoint_coop(const G& grp, const double* th, double* g) const
+    {
+      const double la = ::log(th[0]);
+      double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      for (int i = grp.rank(); i < nbins; i += grp.size()) {
+        const double lx = bins[4 * i], l1 = bins[4 * i + 1];
+        const double k = bins[4 * i + 2], lgk = bins[4 * i + 3];
+        const double ll = la + fma(th[1], l1, -fma(th[3], lx, th[2]) * lx);
+        const double lam = ::exp(ll);
+        v[0] += lam - fma(k, ll, -lgk);
+        const double w = lam - k;
+        v[1] += w;
+        v[2] = fma(w, l1, v[2]);
+        v[3] = fma(-w, lx, v[3]);
+        v[4] = fma(-w * lx, lx, v[4]);
+      }
+      grp.template sum<5>(v);
+      if (grp.rank() == 0) {
+        g[0] = v[1] / th[0];
+        g[1] = v[2];
+        g[2] = v[3];
+        g[3] = v[4];
+      }
+      return v[0];
     }
   };
 
