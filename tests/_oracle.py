@@ -10,6 +10,7 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent.parent
 ORACLE_SO = ROOT / "oracle" / "libzeus_oracle.so"
+ORACLE_FMA_SO = ROOT / "oracle" / "libzeus_oracle_fma.so"
 REF_SO = ROOT / "oracle" / "_ref" / "libzeus_ref.so"
 
 _P = C.c_void_p
@@ -54,6 +55,20 @@ def oracle():
                                    _P, _P, _P, _P]
         _oracle = L
     return _oracle
+
+
+_oracle_fma = None
+
+
+def oracle_fma_bfgs(*a, **k):
+    """The oracle compiled with FMA contraction (the reference's algorithm
+    under an FMA-contracting compiler)."""
+    global _oracle_fma
+    if _oracle_fma is None:
+        L = C.CDLL(str(ORACLE_FMA_SO))
+        L.zor_bfgs.argtypes = _BFGS_SIG
+        _oracle_fma = L
+    return run_bfgs(_oracle_fma.zor_bfgs, *a, **k)
 
 
 def ref_available() -> bool:

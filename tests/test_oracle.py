@@ -290,3 +290,22 @@ def test_update_hoisted_equals_reference_quartic_loop():
             O.oracle().zor_bfgs_update(dim, Ho.ctypes.data, s.ctypes.data, y.ctypes.data, sy)
             O.ref().zref_bfgs_update(dim, Hr.ctypes.data, s.ctypes.data, y.ctypes.data, sy)
             np.testing.assert_array_equal(Ho, Hr)
+
+
+# ---- the reference's own sensitivity to rounding --------------------------
+@pytest.mark.parametrize("kind,dim,lo,hi,n,iters", [
+    (RAS, 2, -5.12, 5.12, 256, 3000), (ACK, 30, -32.768, 32.768, 32, 2000),
+    (ROS, 8, -5, 5, 96, 2000)])
+def test_reference_outcomes_move_with_fma_contraction(kind, dim, lo, hi, n, iters):
+    """The same algorithm with and without FMA contraction (the reference
+    built by nvcc vs for the host) ends some runs differently: run status is
+    not reproducible across compilers, only its statistics and the values of
+    runs both sides converge."""
+    st = O.oracle_starts(21, n, dim, lo, hi)
+    a = O.oracle_bfgs(kind, dim, st, max_iter=iters, lower=lo, upper=hi)
+    b = O.oracle_fma_bfgs(kind, dim, st, max_iter=iters, lower=lo, upper=hi)
+    agree = (a["status"] == b["status"]).mean()
+    both = (a["status"] == 1) & (b["status"] == 1)
+    print(f"kind {kind} dim {dim}: status agreement {agree:.1%}")
+    assert 0.8 <= agree < 1.0
+    assert np.abs(a["fval"][both] - b["fval"][both]).max() <= 1e-8

@@ -138,8 +138,9 @@ namespace zb {
       return;
     const int64_t i = e / dim;
     const int d = (int)(e - i * dim);
-    out[e] =
-      lower + (upper - lower) * uniform01(seed, kTagStarts, (uint64_t)i, d);
+    // no contraction: the same bits as lower + (upper - lower) * u in C
+    out[e] = __dadd_rn(lower, __dmul_rn(upper - lower,
+                                        uniform01(seed, kTagStarts, (uint64_t)i, d)));
   }
 
   __global__ void __launch_bounds__(256)
