@@ -99,26 +99,85 @@ def algorithmic_flops(jobs_counters) -> float:
 
 # ---------------------------------------------------------------- workloads
 class Job:
-    def __init__(self, name, obj_fn, n, lo, hi, pso_iter, max_iter, required, tol=1e-8):
+    """One class of a workload: objective, runs, bounds, PSO iterations (<0:
+    uniform starts), BFGS settings, and the layout used when the class runs
+    in a persistent batch."""
+
+    def __init__(self, name, obj_fn, n, lo, hi, pso_iter, max_iter, required, tol=1e-8,
+                 runs_per_instance=0):
         self.name, self.obj_fn, self.n = name, obj_fn, n
         self.lo, self.hi, self.pso_iter = lo, hi, pso_iter
         self.max_iter, self.required, self.tol = max_iter, required, tol
+        self.runs_per_instance = runs_per_instance
+
+
+def dijet_objective(toys=512, nbins=100, seed=7):
+    """512 Poisson toy spectra of the dijet shape, stored one after another
+    (the batch's per-instance data): 100 log-spaced bins in x = m/13000 over
+    [0.085, 0.54], lambda = p0 (1-x)^p1 / x^(p2 + p3 ln x), p = (1e6, 10, 5,
+    0.1) scaled to 1e6 events."""
+    import zeus_b200 as zb
+
+    edges = np.geomspace(0.085, 0.54, nbins + 1)
+    x = 0.5 * (edges[1:] + edges[:-1])
+    lam = (1 - x) ** 10.0 / x ** (5.0 + 0.1 * np.log(x))
+    lam *= 1e6 / lam.sum()
+    rng = np.random.default_rng(seed)
+    k = rng.poisson(np.tile(lam, (toys, 1))).astype(np.int32)
+    obj = zb.PoissonNLL(k.reshape(-1), np.tile(x, toys))
+    return obj
 
 
 def workloads():
     import zeus_b200 as zb
 
     return {
+        "mixed": dict(
+            desc="uneven persistent batch: 8192 runs, Rosenbrock D in {2,8,32,64,128} "
+                 "(1366,1366,1365,1365,1365) + Ackley-30 (1365), uniform starts "
+                 "(Philox, seed 42 + class), PSO off, <=10000 iters, tol 1e-8, "
+                 "stop-early off",
+            batch=True,
+            jobs=[Job("rosenbrock128", lambda: zb.Rosenbrock(128), 1365, -5.0, 5.0, -1,
+                      10000, 1 << 30),
+                  Job("rosenbrock64", lambda: zb.Rosenbrock(64), 1365, -5.0, 5.0, -1,
+                      10000, 1 << 30),
+                  Job("ackley30", lambda: zb.Ackley(30), 1365, -32.768, 32.768, -1,
+                      10000, 1 << 30),
+                  Job("rosenbrock32", lambda: zb.Rosenbrock(32), 1365, -5.0, 5.0, -1,
+                      10000, 1 << 30),
+                  Job("rosenbrock8", lambda: zb.Rosenbrock(8), 1366, -5.0, 5.0, -1,
+                      10000, 1 << 30),
+                  Job("rosenbrock2", lambda: zb.Rosenbrock(2), 1366, -5.0, 5.0, -1,
+                      10000, 1 << 30)]),
+        "gaussian150": dict(
+            desc="150-D Gaussian 0.5 x^T C x, C_ii = 75.5, C_ij = 0.5, 1024 starts, "
+                 "PSO 10, <=10000 iters, tol 1e-8, stop-early off",
+            batch=False,
+            jobs=[Job("gaussian150", lambda: zb.Gaussian(zb.gaussian_matrix(150)), 1024,
+                      -5.0, 5.0, 10, 10000, 1 << 30)]),
+        "multimodal": dict(
+            desc="Rastrigin-10 (A=10) 16384 starts in +-5.12 and Ackley-30 16384 starts "
+                 "in +-32.768, PSO 20 each (CUDA graph), <=10000 iters, tol 1e-8, "
+                 "stop-early off; both classes in one persistent batch",
+            batch=True,
+            jobs=[Job("ackley30", lambda: zb.Ackley(30), 16384, -32.768, 32.768, 20, 10000,
+                      1 << 30),
+                  Job("rastrigin10", lambda: zb.Rastrigin(10), 16384, -5.12, 5.12, 20,
+                      10000, 1 << 30)]),
+        "dijet": dict(
+            desc="512 Poisson toy dijet spectra x 256 uniform starts in [0,10]^4, "
+                 "4-parameter NLL, one persistent batch of 131072 runs, <=10000 iters, "
+                 "tol 1e-8, stop-early off",
+            batch=True,
+            jobs=[Job("dijet", lambda: dijet_objective(), 131072, 0.0, 10.0, -1, 10000,
+                      1 << 30, runs_per_instance=256)]),
         "rosenbrock2": dict(
             desc="2-D Rosenbrock, 1024 starts, PSO 10, <=10000 BFGS iters, "
                  "required_convergences 100, tol 1e-8, seed 42",
+            batch=False,
             jobs=[Job("rosenbrock2", lambda: zb.Rosenbrock(2), 1024, -5.0, 5.0, 10,
                       10000, 100)]),
-        "rosenbrock2-nostop": dict(
-            desc="2-D Rosenbrock, 1024 starts, PSO 10, <=10000 BFGS iters, "
-                 "stop-early off, tol 1e-8, seed 42",
-            jobs=[Job("rosenbrock2", lambda: zb.Rosenbrock(2), 1024, -5.0, 5.0, 10,
-                      10000, 1025)]),
     }
 
 
@@ -206,10 +265,12 @@ def measure_fp64_peak(torch, zb):
 
 
 def run_gpu(args, rank, world, local_rank):
-    import torch
-    import zeus_b200 as zb
-    from zeus_b200.device import DeviceProblem, BfgsRun, _stream_handle
     import ctypes as C
+
+    import torch
+
+    import zeus_b200 as zb
+    from zeus_b200.device import Batch, BatchJob, BfgsRun, DeviceProblem
 
     torch.cuda.set_device(local_rank)
     wl = workloads()[args.workload]
@@ -221,59 +282,75 @@ def run_gpu(args, rank, world, local_rank):
     torch.cuda.set_stream(stream)
     sh = stream.cuda_stream
     seed = args.seed + 1000003 * rank
+    L = zb.lib()
 
-    # per job: device problem, buffers
     state = []
-    for j in jobs:
+    for ci, j in enumerate(jobs):
         obj = j.obj_fn()
         dp = DeviceProblem(obj, dev)
-        cfg = zb.make_config(j.max_iter, j.required, j.tol, "fast", args.gradient)
-        run = BfgsRun(dp, j.n, cfg, device=dev, counters=True)
-        pws = zb.lib().zeus_pso_workspace_size(j.n, obj.dim)
-        pso = dict(pbx=torch.empty((j.n, obj.dim), dtype=torch.float64, device=dev),
-                   pbf=torch.empty((j.n,), dtype=torch.float64, device=dev),
-                   gb=torch.empty((obj.dim + 1,), dtype=torch.float64, device=dev),
-                   ws=torch.empty((max(pws, 1),), dtype=torch.uint8, device=dev), wsz=pws)
-        cen = torch.zeros((6,), dtype=torch.int32, device=dev)
-        nbins = 0 if obj.idata is None else len(obj.idata)
-        state.append(dict(job=j, obj=obj, dp=dp, run=run, pso=pso, cen=cen, nbins=nbins))
+        d = obj.dim
+        starts = torch.empty((j.n, d), dtype=torch.float64, device=dev)
+        s = dict(job=j, obj=obj, dp=dp, starts=starts, seed=seed + ci,
+                 cen=torch.zeros((6,), dtype=torch.int32, device=dev),
+                 nbins=0 if obj.idata is None else len(obj.idata) // max(
+                     1, (j.n + j.runs_per_instance - 1) // j.runs_per_instance
+                     if j.runs_per_instance else 1))
+        if j.pso_iter >= 0:
+            pws = L.zeus_pso_workspace_size(j.n, d)
+            s["pso"] = dict(pbf=torch.empty((j.n,), dtype=torch.float64, device=dev),
+                            gb=torch.empty((d + 1,), dtype=torch.float64, device=dev),
+                            ws=torch.empty((max(pws, 1),), dtype=torch.uint8, device=dev),
+                            wsz=pws)
+        s["bj"] = BatchJob(dp, starts, required=j.required, runs_per_instance=j.runs_per_instance)
+        if not j.runs_per_instance:
+            cfg_fast = zb.make_config(j.max_iter, j.required, j.tol, "fast", "adjoint")
+            s["run"] = BfgsRun(dp, j.n, cfg_fast, device=dev)
+        state.append(s)
+    batch = Batch([s["bj"] for s in state], jobs[0].max_iter, jobs[0].tol) if wl["batch"] else None
 
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    def gen_starts(s):
+        j, prob = s["job"], s["dp"].c()
+        if j.pso_iter >= 0:
+            p = s["pso"]
+            zb.check(L.zeus_pso_device(C.byref(prob), s["seed"], j.n, j.lo, j.hi, j.pso_iter,
+                                       0.5, 1.2, 1.5, s["starts"].data_ptr(),
+                                       p["pbf"].data_ptr(), p["gb"].data_ptr(),
+                                       p["ws"].data_ptr(), p["wsz"], sh))
+            return 2 + j.pso_iter
+        zb.check(L.zeus_starts_uniform(s["seed"], j.n, s["obj"].dim, j.lo, j.hi,
+                                       s["starts"].data_ptr(), sh))
+        return 1
 
-    def step(timing):
-        ev = []
-        launches = 0
-        for s in state:
-            j, run, p = s["job"], s["run"], s["pso"]
-            prob = s["dp"].c()
-            if j.pso_iter >= 0:
-                zb.check(zb.lib().zeus_pso_device(
-                    C.byref(prob), seed, j.n, j.lo, j.hi, j.pso_iter, 0.5, 1.2, 1.5,
-                    p["pbx"].data_ptr(), p["pbf"].data_ptr(), p["gb"].data_ptr(),
-                    p["ws"].data_ptr(), p["wsz"], sh))
-                launches += 2 + j.pso_iter
-                starts = p["pbx"]
-            else:
-                zb.check(zb.lib().zeus_starts_uniform(seed, j.n, s["obj"].dim, j.lo, j.hi,
-                                                      p["pbx"].data_ptr(), sh))
-                launches += 1
-                starts = p["pbx"]
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            run.launch(starts, stream=stream)
-            e1.record(stream)
-            launches += 1 + (1 if s["nbins"] else 0)
-            ev.append((e0, e1))
-            zb.check(zb.lib().zeus_census_device(
-                run.fval.data_ptr(), run.status.data_ptr(), run.x.data_ptr(), j.n,
-                s["obj"].dim, None, s["cen"].data_ptr(), sh))
-            launches += 1
-        return ev, launches
+    def census(s, out):
+        zb.check(L.zeus_census_device(out.fval.data_ptr(), out.status.data_ptr(),
+                                      out.x.data_ptr(), s["job"].n, s["obj"].dim, None,
+                                      s["cen"].data_ptr(), sh))
+        return 1
 
-    # warm-up
+    def step_fast():
+        """The adjoint + persistent-batched form; returns (events, launches)."""
+        launches = sum(gen_starts(s) for s in state)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if batch is not None:
+            batch.launch(stream)
+            launches += 1 + sum(1 for s in state if s["nbins"])
+            outs = [s["bj"] for s in state]
+        else:
+            for s in state:
+                s["run"].launch(s["starts"], stream=stream)
+                launches += 1 + (1 if s["nbins"] else 0)
+            outs = [s["run"] for s in state]
+        e1.record(stream)
+        for s, o in zip(state, outs):
+            launches += census(s, o)
+        return (e0, e1), launches, outs
+
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.float32, device=dev)
+
     for _ in range(args.warmup):
-        step(False)
+        step_fast()
     torch.cuda.synchronize()
 
     clocks = ClockSampler(local_rank)
@@ -281,28 +358,38 @@ def run_gpu(args, rank, world, local_rank):
         clocks.start()
         clocks.wait_samples(1)
     times, kern_ms, conv, launches = [], [], [], 0
-    counters = []
+    outs = None
     for k in range(args.steps):
-        flush.zero_()  # write 1 GiB: larger than the 126 MB L2
+        flush.zero_()  # 1 GiB written: larger than the 126 MB L2
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         t0.record(stream)
-        ev, nl = step(True)
+        (e0, e1), nl, outs = step_fast()
         t1.record(stream)
         torch.cuda.synchronize()
         launches += nl
         times.append(t0.elapsed_time(t1))
-        kern_ms.append(sum(a.elapsed_time(b) for a, b in ev))
+        kern_ms.append(e0.elapsed_time(e1))
         conv.append(sum(int(s["cen"][1].item()) for s in state))
-        counters = [((s["obj"].kind, s["obj"].dim, args.gradient, s["nbins"]),
-                     s["run"].counters.cpu().numpy()) for s in state]
     if rank == 0:
-        n0 = len(clocks.rows)
-        clocks.wait_samples(n0 + 1)  # one sample after the last timed step
+        clocks.wait_samples(len(clocks.rows) + 1)
         clocks.stop()
+    counters = [((s["obj"].kind, s["obj"].dim, "adjoint", max(s["nbins"], 100)),
+                 o.counters.cpu().numpy()) for s, o in zip(state, outs)]
+    iters_per_class = [o.iter.cpu().numpy() for o in outs]
+    status_per_class = [o.status.cpu().numpy() for o in outs]
+    if args.write_iterations and rank == 0:
+        path = Path(args.write_iterations)
+        doc = json.loads(path.read_text()) if path.exists() else {}
+        doc[args.workload] = {
+            s["job"].name: {"mean_iterations": float(np.mean(it)),
+                            "converged_fraction": float(np.mean(st == 1)),
+                            "runs": int(len(it))}
+            for s, it, st in zip(state, iters_per_class, status_per_class)}
+        path.write_text(json.dumps(doc, indent=1, sort_keys=True) + "\n")
 
     step_ms = float(np.mean(times))
     conv_mean = float(np.mean(conv))
@@ -317,30 +404,99 @@ def run_gpu(args, rank, world, local_rank):
         step_ms_all, conv_all = step_ms, conv_mean
     value = conv_all / (step_ms_all * 1e-3)
 
-    # roofline: the BFGS kernel, FP64 work per launch / its event time
     flops = algorithmic_flops(counters)
     kms = float(np.mean(kern_ms))
     achieved = flops / (kms * 1e-3) / 1e12
     peak = measure_fp64_peak(torch, zb) if rank == 0 else None
 
-    # e2e through the host-buffer C-ABI call
-    e2e_ms, e2e_conv = [], []
-    h2d = sum(0 if s["obj"].data is None else s["obj"].data.nbytes +
-              (0 if s["obj"].idata is None else s["obj"].idata.nbytes) for s in state)
-    d2h = sum(24 + 24 + 8 * s["obj"].dim for s in state)
-    for k in range(args.warmup + args.steps):
-        t_a = time.perf_counter()
-        cc = 0
+    # the plain form: dual-number gradients, one standalone launch per class
+    plain = None
+    if not args.no_plain:
+        pl_runs = []
         for s in state:
             j = s["job"]
-            r = zb.Zeus(s["obj"], j.lo, j.hi, j.n, j.max_iter, j.pso_iter, j.required,
-                        j.name, j.tol, seed, 0, gradient=args.gradient,
-                        stream=sh)
-            cc += r.c.claimed
+            if j.runs_per_instance:
+                pj = BatchJob(s["dp"], s["starts"], required=j.required,
+                              runs_per_instance=j.runs_per_instance)
+                pl_runs.append(("batchjob", pj))
+            else:
+                cfg_pl = zb.make_config(j.max_iter, j.required, j.tol, "fast", "dual")
+                pl_runs.append(("run", BfgsRun(s["dp"], j.n, cfg_pl, device=dev)))
+        pl_t, pl_c = [], []
+        for k in range(1 + args.plain_steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for s in state:
+                gen_starts(s)
+            for s, (kind, r) in zip(state, pl_runs):
+                if kind == "run":
+                    r.launch(s["starts"], stream=stream)
+                    census(s, r)
+                else:
+                    # per-instance data: standalone launches cannot carry it,
+                    # the batch kernel's single class with dual gradients
+                    # would be needed; dijet has no plain form here
+                    pass
+            t1.record(stream)
+            torch.cuda.synchronize()
+            if k >= 1:
+                pl_t.append(t0.elapsed_time(t1))
+                pl_c.append(sum(int(s["cen"][1].item()) for s, (kd, _) in
+                                zip(state, pl_runs) if kd == "run"))
+        if all(kd == "run" for kd, _ in pl_runs):
+            pv = float(np.mean(pl_c)) / (float(np.mean(pl_t)) * 1e-3)
+            plain = {"value": pv, "unit": "runs/s", "ms_per_step": float(np.mean(pl_t)),
+                     "converged_per_step": float(np.mean(pl_c)),
+                     "form": "dual-number gradients, one standalone launch per class, "
+                             "default layout by dimension",
+                     "speedup_of_headline": value / pv if pv > 0 else None}
+
+    # e2e: pinned host inputs -> device, the same step, D2H of the census
+    e2e_ms, e2e_conv = [], []
+    host_inputs = []
+    for s in state:
+        hi = {}
+        if s["job"].pso_iter < 0:
+            hi["starts"] = s["starts"].cpu().pin_memory()
+        if s["dp"].data is not None:
+            hi["data"] = s["dp"].data.cpu().pin_memory()
+        if s["dp"].idata is not None:
+            hi["idata"] = s["dp"].idata.cpu().pin_memory()
+        host_inputs.append(hi)
+    h2d = sum(t.numel() * t.element_size() for hi in host_inputs for t in hi.values())
+    cen_host = torch.zeros((len(state), 6), dtype=torch.int32).pin_memory()
+    d2h = cen_host.numel() * 4
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t_a = time.perf_counter()
+        for s, hi in zip(state, host_inputs):
+            if "starts" in hi:
+                s["starts"].copy_(hi["starts"], non_blocking=True)
+            if "data" in hi:
+                s["dp"].data.copy_(hi["data"], non_blocking=True)
+            if "idata" in hi:
+                s["dp"].idata.copy_(hi["idata"], non_blocking=True)
+        for s in state:
+            if s["job"].pso_iter >= 0:
+                gen_starts(s)
+        if batch is not None:
+            batch.launch(stream)
+            o2 = [s["bj"] for s in state]
+        else:
+            for s in state:
+                s["run"].launch(s["starts"], stream=stream)
+            o2 = [s["run"] for s in state]
+        for i, (s, o) in enumerate(zip(state, o2)):
+            census(s, o)
+            cen_host[i].copy_(s["cen"], non_blocking=True)
+        stream.synchronize()
         t_b = time.perf_counter()
         if k >= args.warmup:
             e2e_ms.append((t_b - t_a) * 1e3)
-            e2e_conv.append(cc)
+            e2e_conv.append(int(cen_host[:, 1].sum()))
     e2e_val = float(np.mean(e2e_conv)) / (float(np.mean(e2e_ms)) * 1e-3)
     if world > 1:
         t = torch.tensor([e2e_val], dtype=torch.float64, device=dev)
@@ -349,11 +505,11 @@ def run_gpu(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args, state, torch)
+        cpu = cpu_baseline(args, state, iters_per_class, status_per_class)
 
     if rank == 0:
         line = {
-            "metric": "converged runs/s at ||grad||<1e-8 (adjoint+batched form)",
+            "metric": "converged runs/s at ||grad||<1e-8 (adjoint+persistent-batched form)",
             "value": value,
             "unit": "runs/s",
             "n_gpus": world,
@@ -366,17 +522,20 @@ def run_gpu(args, rank, world, local_rank):
             "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": args.workload, "description": wl["desc"],
-                       "gradient": args.gradient, "mode": "fast",
+                       "gradient": "adjoint", "mode": "fast",
+                       "batched": bool(wl["batch"]),
                        "converged_per_step": conv_all,
+                       "runs_per_step": sum(j.n for j in jobs) * world,
                        "l2": "1 GiB buffer written between timed steps",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-            "roofline": {"bound": "fp64", "kernel": "bfgs (all BFGS launches of a step)",
+            "plain_dual": plain,
+            "roofline": {"bound": "fp64", "kernel": "bfgs_batch_kernel" if batch is not None
+                         else "bfgs (standalone launches)",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": (achieved / peak) if peak else None,
                          "peak_source": "measured FP64 FMA probe on this GPU "
                                         "(zeus_probe_fp64)",
-                         "flops_per_step": flops, "kernel_ms": kms,
-                         "traffic": None},
+                         "flops_per_step": flops, "kernel_ms": kms, "traffic": None},
             "e2e": {"value": e2e_val, "unit": "runs/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": float(np.mean(e2e_ms))},
             "gpu_launches": launches,
@@ -412,31 +571,77 @@ def _ref_lib():
     return O, None
 
 
-def cpu_baseline(args, state, torch):
-    """The reference's sequential BFGS (host build) on the same starts as the
-    GPU's last step, all host threads."""
+ITERS_FIXTURE = ROOT / "tests" / "golden" / "workload_iterations.json"
+# per class: runs of the reference's sequential BFGS timed to completion,
+# or (heavy classes, where one run can take minutes) iterations per run
+# timed on one run per core and scaled by the workload's iteration counts
+FULL_SAMPLE = {2: 1024, 4: 256, 8: 128, 10: 128, 16: 64, 30: 16, 32: 16}
+ITER_SAMPLE = {64: 20, 128: 4, 150: 5}
+
+
+def _class_sample(O, obj, job, starts_host, cores, iters=None, statuses=None):
+    """Estimated (converged runs, core-seconds) of the whole class on the
+    reference host build, and a description of the sample."""
+    d = obj.dim
+    n = job.n
+    data, idata = obj.data, obj.idata
+    if job.runs_per_instance:  # one data instance (the first toy)
+        nb = len(obj.idata) // ((n + job.runs_per_instance - 1) // job.runs_per_instance)
+        data, idata = obj.data[:nb], obj.idata[:nb]
+    if d in ITER_SAMPLE:
+        m = ITER_SAMPLE[d]
+        k = min(cores, n)
+        with _QuietStdout():
+            t0 = time.perf_counter()
+            O.ref_bfgs(obj.kind, d, starts_host[:k], max_iter=m, required=1 << 30,
+                       tol=job.tol, data=data, idata=idata, lower=job.lo, upper=job.hi,
+                       nthreads=cores)
+            wall = time.perf_counter() - t0
+        t_iter = wall / m  # seconds per iteration on one core (k runs in parallel)
+        if iters is None:
+            return None, None, "no iteration counts"
+        core_s = float(np.sum(np.maximum(iters, 1))) * t_iter
+        conv = float((statuses == 1).sum())
+        return conv, core_s, (f"{job.name}: {k} runs x {m} iterations timed "
+                              f"({t_iter * 1e3:.1f} ms/iteration/core), scaled by the "
+                              f"workload's {int(np.sum(iters))} iterations")
+    k = min(FULL_SAMPLE.get(d, 64), n)
+    with _QuietStdout():
+        t0 = time.perf_counter()
+        r = O.ref_bfgs(obj.kind, d, starts_host[:k], max_iter=job.max_iter,
+                       required=job.required, tol=job.tol, data=data, idata=idata,
+                       lower=job.lo, upper=job.hi, nthreads=cores)
+        wall = time.perf_counter() - t0
+    conv = float((r["status"] == 1).sum()) * n / k
+    core_s = wall * cores * n / k
+    return conv, core_s, f"{job.name}: {k} of {n} runs to completion"
+
+
+def cpu_baseline(args, state, iters_per_class, status_per_class):
+    """The reference's sequential BFGS (host build, all host threads) on a
+    bounded sample of this workload, same starts as the GPU's last step."""
     O, why = _ref_lib()
     if O is None:
         return {"value": None, "unit": "runs/s", "cores": 0, "kind": "reference",
                 "sample": why}
     cores = os.cpu_count() or 1
-    total_t, total_conv, sample = 0.0, 0, []
-    for s in state:
-        j, obj = s["job"], s["obj"]
-        starts = s["pso"]["pbx"].cpu().numpy()
-        with _QuietStdout():
-            t0 = time.perf_counter()
-            r = O.ref_bfgs(obj.kind, obj.dim, starts, max_iter=j.max_iter,
-                           required=j.required, tol=j.tol, data=obj.data, idata=obj.idata,
-                           lower=j.lo, upper=j.hi, nthreads=cores)
-            total_t += time.perf_counter() - t0
-        total_conv += int((r["status"] == 1).sum())
-        sample.append(f"{j.name}: all {j.n} runs from the GPU's PSO starts")
-    return {"value": total_conv / total_t, "unit": "runs/s", "cores": cores,
-            "kind": "reference", "sample": "; ".join(sample), "seconds": total_t}
+    conv, core_s, desc = 0.0, 0.0, []
+    for s, it, st in zip(state, iters_per_class, status_per_class):
+        c, cs, dsc = _class_sample(O, s["obj"], s["job"], s["starts"].cpu().numpy(), cores,
+                                   it, st)
+        conv += c
+        core_s += cs
+        desc.append(dsc)
+    wall = core_s / cores
+    return {"value": conv / wall, "unit": "runs/s", "cores": cores, "kind": "reference",
+            "sample": "; ".join(desc), "estimated_seconds_for_workload": wall}
 
 
 def run_reference(args, rank, world):
+    """The reference's own CPU implementation of the path (its sequential BFGS
+    built for the host) on the same workload, all host threads.  Heavy
+    classes are timed per iteration and scaled by the workload's per-run
+    iteration counts recorded in tests/golden/workload_iterations.json."""
     if rank != 0:
         return
     O, why = _ref_lib()
@@ -444,43 +649,53 @@ def run_reference(args, rank, world):
     if O is None:
         print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
         return
+    fixture = {}
+    if ITERS_FIXTURE.exists():
+        fixture = json.loads(ITERS_FIXTURE.read_text()).get(args.workload, {})
     cores = os.cpu_count() or 1
-    # starts: the oracle's synchronous PSO restatement with the same seed
     sts = []
-    for j in wl["jobs"]:
+    for ci, j in enumerate(wl["jobs"]):
         obj = j.obj_fn()
+        seed = args.seed + ci
         if j.pso_iter >= 0:
-            pbx, _, _, _ = O.oracle_pso(obj.kind, obj.dim, args.seed, j.n, j.lo, j.hi,
-                                        j.pso_iter, data=obj.data, idata=obj.idata)
+            pbx, _, _, _ = O.oracle_pso(obj.kind, obj.dim, seed, j.n, j.lo, j.hi,
+                                        j.pso_iter, data=obj.data if obj.kind == 3 else None)
         else:
-            pbx = O.oracle_starts(args.seed, j.n, obj.dim, j.lo, j.hi)
+            pbx = O.oracle_starts(seed, min(j.n, 4096), obj.dim, j.lo, j.hi)
         sts.append((j, obj, pbx))
-    times, convs = [], []
+    times, convs, desc = [], [], []
     for k in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        c = 0
+        conv, core_s, desc = 0.0, 0.0, []
         for j, obj, pbx in sts:
-            with _QuietStdout():
-                r = O.ref_bfgs(obj.kind, obj.dim, pbx, max_iter=j.max_iter,
-                               required=j.required, tol=j.tol, data=obj.data,
-                               idata=obj.idata, lower=j.lo, upper=j.hi, nthreads=cores)
-            c += int((r["status"] == 1).sum())
-        dt = time.perf_counter() - t0
+            fx = fixture.get(j.name)
+            it = st = None
+            if fx is not None:
+                it = np.full(j.n, fx["mean_iterations"])
+                st = np.zeros(j.n, np.int32)
+                st[:int(round(fx["converged_fraction"] * j.n))] = 1
+            c, cs, dsc = _class_sample(O, obj, j, pbx, cores, it, st)
+            if c is None:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  f"{j.name}: per-run iteration counts missing from "
+                                  f"{ITERS_FIXTURE.name}"}), flush=True)
+                return
+            conv += c
+            core_s += cs
+            desc.append(dsc)
         if k >= args.warmup:
-            times.append(dt)
-            convs.append(c)
+            times.append(core_s / cores)
+            convs.append(conv)
     v = float(np.mean(convs)) / float(np.mean(times))
     print(json.dumps({
         "impl": "reference",
-        "metric": "converged runs/s at ||grad||<1e-8 (adjoint+batched form)",
+        "metric": "converged runs/s at ||grad||<1e-8 (adjoint+persistent-batched form)",
         "value": v, "unit": "runs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": float(np.mean(times)) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "description": wl["desc"]},
         "cpu_baseline": {"value": v, "unit": "runs/s", "cores": cores, "kind": "reference",
-                         "sample": "whole workload per step; starts from the synchronous "
-                                   "PSO restatement (same seed)"},
+                         "sample": "; ".join(desc)},
         "e2e": {"value": v, "unit": "runs/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -493,10 +708,15 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="zeus_b200", choices=["zeus_b200", "reference"])
-    ap.add_argument("--workload", default="rosenbrock2")
+    ap.add_argument("--workload", default="mixed")
     ap.add_argument("--gradient", default="adjoint", choices=["adjoint", "dual"])
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="skip the plain dual-AD comparison")
+    ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--write-iterations", default="",
+                    help="write per-class iteration statistics (for the reference arm)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

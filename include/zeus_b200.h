@@ -186,6 +186,56 @@ int zeus_bfgs_device(const zeus_problem* problem,
                      int32_t* d_control, void* d_workspace,
                      size_t workspace_bytes, void* stream);
 
+/* ---- persistent batch -----------------------------------------------
+ * No single reference counterpart: the reference runs one objective per
+ * zeus::Zeus call (zeus.cuh:341-375), one kernel launch per call.  This
+ * runs up to 16 classes -- each an objective and dimension with its own
+ * runs, starts, outputs and stop-early control, as one Zeus call would --
+ * in ONE persistent kernel launch.  Slots are refilled from per-class
+ * atomic queues as runs finish; CTA-layout classes (dim > 32) go first,
+ * biggest first.  A class may carry several data instances stored one
+ * after another (Gaussian: dim*dim doubles each; NLL: ndata centres and
+ * ndata counts each), run r using instance r / runs_per_instance.
+ * Fast mode with adjoint gradients only (config->mode, ->gradient);
+ * config->max_iter, ->tolerance and ->flags apply to every class. */
+typedef struct zeus_batch_class {
+  zeus_problem problem;       /* data on the device */
+  int64_t n;                  /* runs */
+  int64_t runs_per_instance;  /* 0: every run uses the one instance */
+  const double* d_starts;     /* n*dim, row-major */
+  zeus_run_outputs out;       /* per-run outputs (trajectories ignored) */
+  int32_t* d_control;         /* 2 int32 {stop, converged}, zeroed */
+  int32_t required_converged; /* stop-early threshold of this class */
+  int32_t layout;             /* ZEUS_LAYOUT_* (AUTO: autotuned/default) */
+  int32_t tile;               /* tile width for ZEUS_LAYOUT_TILE */
+  int32_t reserved;
+} zeus_batch_class;
+
+size_t zeus_batch_workspace_size(const zeus_batch_class* classes,
+                                 int32_t n_classes);
+int zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
+                      const zeus_bfgs_config* config, void* d_workspace,
+                      size_t workspace_bytes, void* stream);
+
+/* ---- layout autotuner -------------------------------------------------
+ * No reference counterpart (the reference fixes thread-per-run or a tile
+ * of min(32, 2^floor(log2 D)) lanes, bfgs_parallel.cuh:57-65).  Times every
+ * built layout / tile width for (problem, config) on n_sample uniform
+ * starts in [lower, upper) and records the fastest in a per-process table
+ * keyed by (device, kind, dim, gradient); ZEUS_LAYOUT_AUTO launches and
+ * batches then use it.  Synchronous.  *best_ms is the winner's time. */
+int zeus_autotune(const zeus_problem* problem, const zeus_bfgs_config* config,
+                  int64_t n_sample, uint64_t seed, double lower, double upper,
+                  int32_t* best_layout, int32_t* best_tile, float* best_ms,
+                  void* stream);
+/* 1 and the recorded choice if (kind, dim, gradient) is in the table for
+ * the current device, else 0. */
+int zeus_autotune_lookup(int32_t kind, int32_t dim, int32_t gradient,
+                         int32_t* layout, int32_t* tile);
+/* Records a choice (e.g. from a previous process) for the current device. */
+int zeus_autotune_record(int32_t kind, int32_t dim, int32_t gradient,
+                         int32_t layout, int32_t tile);
+
 /* ---- reduction ------------------------------------------------------
  * Replaces bfgs::launchReduction + util::dumpDataToFile's census
  * (bfgs_common.cuh:280-319, util.hpp:151-200): argmin of fval (lowest index

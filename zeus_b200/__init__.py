@@ -107,6 +107,21 @@ class CCensus(C.Structure):
     ]
 
 
+class BatchClass(C.Structure):
+    _fields_ = [
+        ("problem", Problem),
+        ("n", C.c_int64),
+        ("runs_per_instance", C.c_int64),
+        ("d_starts", C.c_void_p),
+        ("out", RunOutputs),
+        ("d_control", C.c_void_p),
+        ("required_converged", C.c_int32),
+        ("layout", C.c_int32),
+        ("tile", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
 # Every symbol include/zeus_b200.h declares: (name, restype, argtypes).
 _P = C.c_void_p
 SIGNATURES = {
@@ -139,6 +154,18 @@ SIGNATURES = {
          C.c_int32, C.c_int32, C.c_double, C.c_uint64, C.POINTER(BfgsConfig),
          C.POINTER(CResult), _P, C.POINTER(CCensus), _P, _P, _P],
     ),
+    "zeus_batch_workspace_size": (C.c_size_t, [C.POINTER(BatchClass), C.c_int32]),
+    "zeus_batch_device": (
+        C.c_int, [C.POINTER(BatchClass), C.c_int32, C.POINTER(BfgsConfig), _P, C.c_size_t,
+                  _P]),
+    "zeus_autotune": (
+        C.c_int,
+        [C.POINTER(Problem), C.POINTER(BfgsConfig), C.c_int64, C.c_uint64, C.c_double,
+         C.c_double, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_float), _P]),
+    "zeus_autotune_lookup": (
+        C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                  C.POINTER(C.c_int32)]),
+    "zeus_autotune_record": (C.c_int, [C.c_int32] * 5),
     "zeus_probe_fp64_shape": (None, [C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "zeus_probe_fp64": (C.c_int, [C.c_int64, _P, _P]),
 }
@@ -324,10 +351,12 @@ def Zeus(f: Objective, lower: float, upper: float, N: int, MAX_ITER: int,
     return r
 
 
-from .device import bfgs_device, pso_device, starts_uniform, census_device  # noqa: E402
+from .device import (bfgs_device, pso_device, starts_uniform, census_device,  # noqa: E402
+                     batch_device, autotune, BatchJob)
 
 __all__ = [
     "Zeus", "Result", "Convergence", "Objective", "Rosenbrock", "Rastrigin",
     "Ackley", "Gaussian", "PoissonNLL", "gaussian_matrix", "bfgs_device",
     "pso_device", "starts_uniform", "census_device", "lib", "supported",
+    "batch_device", "autotune", "BatchJob",
 ]

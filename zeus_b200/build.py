@@ -41,6 +41,7 @@ UNITS = [
     ("zb_fast_thread.cu", []),
     ("zb_fast_tile.cu", []),
     ("zb_fast_cta.cu", []),
+    ("zb_batch.cu", []),
     ("zb_runtime.cu", []),
 ]
 

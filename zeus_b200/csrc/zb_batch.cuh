@@ -1,0 +1,99 @@
+// Persistent batched BFGS: one launch runs every class of a batch.
+//
+// A class is one (objective, dimension) with its own runs, starts, outputs
+// and stop-early control; classes may have per-instance data (e.g. one toy
+// spectrum per 256 runs).  One block of kBatchBlock threads per SM:
+//
+//   phase A  the block takes runs of the CTA-layout classes (D > 32) one at
+//            a time from each class's atomic queue, biggest dimension first,
+//            and runs each with the whole block (H in shared memory);
+//   phase B  each warp, independently, walks the tile- and thread-layout
+//            classes: its tiles (or single threads) pop runs from the class
+//            queue as their previous run ends, so a slot is refilled the
+//            moment its run converges, stalls or fails.  A warp syncs only
+//            when it moves on to the next class (its tile width may change).
+//
+// The per-run bodies are the standalone layouts' (tile_run, cta_run,
+// thread_run), so results equal the standalone kernels' run for run.
+#pragma once
+
+#include "zb_bfgs_coop.cuh"
+#include "zb_internal.h"
+#include "zb_objectives.cuh"
+
+namespace zb {
+
+  inline constexpr int kBatchBlock = 512;
+
+  struct BatchClass {
+    int kind, dim, layout, tile;
+    int64_t n;
+    const double* starts;
+    RunOut out;
+    Control* ctl;
+    const double* data;
+    const int* idata;
+    int ndata;
+    int flags;
+    const double* nll_bins;
+    int64_t runs_per_instance; // 0: one instance shared by all runs
+    unsigned long long* queue;
+    int required;
+  };
+
+  inline constexpr int kMaxBatchClasses = 16;
+
+  // The whole batch description travels as the kernel's parameter block
+  // (about 2.6 KB): no host-to-device copy, capturable in a CUDA graph.
+  struct BatchTable {
+    int ncls;
+    int max_iter;
+    double tol;
+    int flags;
+    BatchClass c[kMaxBatchClasses];
+  };
+
+  // Tile widths compiled into the batch kernel for a dimension: rows of H
+  // of at most 32 doubles per lane (the kernel is limited to 128 registers
+  // per thread by its 512-thread, one-block-per-SM launch bounds).
+  __host__ __device__ constexpr unsigned
+  batch_widths(int d)
+  {
+    unsigned m = 0;
+    if (d > 32)
+      return 0;
+    for (int k = 1; k <= 5; ++k) {
+      const int ts = 1 << k;
+      const int r = (d + ts - 1) / ts;
+      if (r * d <= 32 && ts <= 2 * d)
+        m |= 1u << k;
+    }
+    return m;
+  }
+  inline constexpr int kBatchThreadMaxDim = 4;
+  inline constexpr int kBatchCtaMinDim = 33;
+
+  // Objective with instance `inst`'s data: instances are stored one after
+  // another (Gaussian: D*D doubles; NLL: ndata centres / counts, 4*ndata
+  // bin constants).
+  template <class F>
+  __device__ __forceinline__ F
+  with_instance(F f, const BatchClass& c, int64_t inst)
+  {
+    if constexpr (requires { f.C; }) {
+      f.C += inst * (int64_t)c.dim * c.dim;
+    } else if constexpr (requires { f.bins; }) {
+      f.centres += inst * c.ndata;
+      f.counts += inst * c.ndata;
+      f.bins += inst * 4 * (int64_t)c.ndata;
+    }
+    return f;
+  }
+
+  __host__ __device__ inline size_t
+  batch_tile_buf_doubles(int dim, int ts)
+  {
+    return (size_t)(32 / ts) * (4 * dim + ts);
+  }
+
+} // namespace zb

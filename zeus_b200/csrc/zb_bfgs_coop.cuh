@@ -92,31 +92,27 @@ namespace zb {
     return 4 * D + TS; // xs, gs, b1, b2, scratch
   }
 
+  // One run on a tile: `buf` is the tile's tile_smem_doubles<D, TS>()
+  // doubles of shared memory; start x0[D]; results to slot `run` of `out`.
   template <class F, int D, int TS, bool Adjoint>
-  __global__ void __launch_bounds__(kTileBlock)
-    bfgs_tile_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
-                     RunOut out, Control* ctl)
+  __device__ __forceinline__ void
+  tile_run(const F& f, cg::thread_block_tile<TS> tile, double* buf,
+           const BfgsParams& prm, const double* __restrict__ x0, int64_t run,
+           const RunOut& out, Control* ctl)
   {
     constexpr int R = (D + TS - 1) / TS;
-    constexpr int TPB = kTileBlock / TS;
-    extern __shared__ double sm[];
-    auto tile = cg::tiled_partition<TS>(cg::this_thread_block());
-    const int tslot = threadIdx.x / TS;
     const int lane = (int)tile.thread_rank();
-    double* xs = sm + tslot * tile_smem_doubles<D, TS>();
+    double* xs = buf;
     double* gs = xs + D;
     double* b1 = gs + D;
     double* b2 = b1 + D;
     TileGroup<TS> grp(tile, b2 + D);
-    const int64_t run = (int64_t)blockIdx.x * TPB + tslot;
-    if (run >= prm.n)
-      return; // the whole tile leaves together
 
     double x[R], g[R], p[R], H[R][D];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int i = lane + r * TS;
-      x[r] = i < D ? starts[run * D + i] : 0.0;
+      x[r] = i < D ? x0[i] : 0.0;
       if (i < D)
         xs[i] = x[r];
 #pragma unroll
@@ -314,6 +310,22 @@ namespace zb {
     }
   }
 
+  template <class F, int D, int TS, bool Adjoint>
+  __global__ void __launch_bounds__(kTileBlock)
+    bfgs_tile_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
+                     RunOut out, Control* ctl)
+  {
+    constexpr int TPB = kTileBlock / TS;
+    extern __shared__ double sm[];
+    auto tile = cg::tiled_partition<TS>(cg::this_thread_block());
+    const int tslot = threadIdx.x / TS;
+    const int64_t run = (int64_t)blockIdx.x * TPB + tslot;
+    if (run >= prm.n)
+      return; // the whole tile leaves together
+    tile_run<F, D, TS, Adjoint>(f, tile, sm + tslot * tile_smem_doubles<D, TS>(),
+                                prm, starts + run * D, run, out, ctl);
+  }
+
   // ---------------------------------------------------------------- CTA
   // Shared-memory layout (doubles): H[D*D] | 11 vectors of D | partial sums
   // 2*Q*D | reduction 32*8 | scratch blockDim | flags (as doubles) 4.
@@ -325,13 +337,15 @@ namespace zb {
     return (size_t)D * D + 11 * D + 2 * q * D + 32 * 8 + block + 4;
   }
 
+  // One run on the whole block (blockDim.x == kBlock): `sm` holds
+  // cta_smem_doubles<D>(kBlock) doubles; start x0[D]; results to slot `run`.
   template <class F, int D, bool Adjoint, int kBlock>
-  __global__ void __launch_bounds__(kBlock)
-    bfgs_cta_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
-                    RunOut out, Control* ctl)
+  __device__ __forceinline__ void
+  cta_run(const F& f, double* sm, const BfgsParams& prm,
+          const double* __restrict__ x0, int64_t run, const RunOut& out,
+          Control* ctl)
   {
     constexpr int Q = kBlock >= D ? kBlock / D : 1;
-    extern __shared__ double sm[];
     double* H = sm;
     double* x = H + D * D;
     double* g = x + D;
@@ -353,9 +367,9 @@ namespace zb {
     const int t = threadIdx.x;
     constexpr bool kTrialGrad = Adjoint && TrialsWithGradient<F>;
 
-    for (int64_t run = blockIdx.x; run < prm.n; run += gridDim.x) {
+    {
       for (int i = t; i < D; i += kBlock)
-        x[i] = starts[run * D + i];
+        x[i] = x0[i];
       for (int e = t; e < D * D; e += kBlock)
         H[e] = (e / D == e % D) ? 1.0 : 0.0;
       __syncthreads();
@@ -544,6 +558,17 @@ namespace zb {
       }
       __syncthreads();
     }
+  }
+
+  template <class F, int D, bool Adjoint, int kBlock>
+  __global__ void __launch_bounds__(kBlock)
+    bfgs_cta_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
+                    RunOut out, Control* ctl)
+  {
+    extern __shared__ double sm[];
+    for (int64_t run = blockIdx.x; run < prm.n; run += gridDim.x)
+      cta_run<F, D, Adjoint, kBlock>(f, sm, prm, starts + run * D, run, out,
+                                     ctl);
   }
 
 } // namespace zb

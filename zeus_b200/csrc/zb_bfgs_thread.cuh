@@ -67,19 +67,17 @@ namespace zb {
     }
   }
 
+  // One run, start x0[D], results to slot idx of `out`.
   template <class F, int D, bool Adjoint>
-  __global__ void __launch_bounds__(128)
-    bfgs_thread_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
-                       RunOut out, Control* ctl)
+  __device__ __forceinline__ void
+  thread_run(const F& f, const BfgsParams& prm, const double* __restrict__ x0,
+             int64_t idx, const RunOut& out, Control* ctl)
   {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= prm.n)
-      return;
     constexpr int NT = D * (D + 1) / 2;
     double x[D], g[D], p[D], H[NT];
 #pragma unroll
     for (int i = 0; i < D; ++i)
-      x[i] = starts[idx * D + i];
+      x[i] = x0[i];
 #pragma unroll
     for (int i = 0; i < D; ++i)
 #pragma unroll
@@ -228,6 +226,16 @@ namespace zb {
       out.counters[3 * idx + 1] = n_eval;
       out.counters[3 * idx + 2] = n_grad;
     }
+  }
+
+  template <class F, int D, bool Adjoint>
+  __global__ void __launch_bounds__(128)
+    bfgs_thread_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
+                       RunOut out, Control* ctl)
+  {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < prm.n)
+      thread_run<F, D, Adjoint>(f, prm, starts + idx * D, idx, out, ctl);
   }
 
 } // namespace zb

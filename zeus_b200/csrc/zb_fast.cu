@@ -63,7 +63,8 @@ namespace zb {
     if (prm.n <= 0)
       return ZEUS_OK;
     int layout = c.layout, tile = c.tile;
-    if (layout == ZEUS_LAYOUT_AUTO)
+    if (layout == ZEUS_LAYOUT_AUTO &&
+        !zeus_autotune_lookup(o.kind, o.dim, c.gradient, &layout, &tile))
       default_layout(o.kind, o.dim, &layout, &tile);
     switch (layout) {
       case ZEUS_LAYOUT_THREAD:

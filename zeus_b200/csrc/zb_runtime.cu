@@ -249,6 +249,18 @@ namespace zb {
                                         : fast_workspace_bytes(o, *c, n);
     }
 
+    // Autotuned layouts: (device, kind, dim, gradient) -> (layout, tile).
+    struct TuneTable {
+      std::mutex mu;
+      std::map<std::tuple<int, int, int, int>, std::pair<int, int>> m;
+    };
+    TuneTable&
+    tune_table()
+    {
+      static TuneTable* t = new TuneTable;
+      return *t;
+    }
+
     // Cached executable graphs for the PSO loop, keyed by the launch shape;
     // new pointer arguments go in through cudaGraphExecUpdate.
     struct GraphCache {
@@ -674,6 +686,156 @@ zeus_optimize(const zeus_problem* hp, double lower, double upper, int64_t n,
   for (void* p : allocs)
     cudaFreeAsync(p, st);
   return cuda_fail(cudaStreamSynchronize(st), "free");
+}
+
+int
+zeus_autotune_lookup(int32_t kind, int32_t dim, int32_t gradient,
+                     int32_t* layout, int32_t* tile)
+{
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess)
+    return 0;
+  TuneTable& t = tune_table();
+  std::lock_guard<std::mutex> lk(t.mu);
+  auto it = t.m.find(std::make_tuple(dev, (int)kind, (int)dim, (int)gradient));
+  if (it == t.m.end())
+    return 0;
+  if (layout)
+    *layout = it->second.first;
+  if (tile)
+    *tile = it->second.second;
+  return 1;
+}
+
+int
+zeus_autotune_record(int32_t kind, int32_t dim, int32_t gradient,
+                     int32_t layout, int32_t tile)
+{
+  if (layout < ZEUS_LAYOUT_THREAD || layout > ZEUS_LAYOUT_CTA) {
+    set_error("zeus_autotune_record: layout must be THREAD, TILE or CTA");
+    return ZEUS_E_INVALID;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  TuneTable& t = tune_table();
+  std::lock_guard<std::mutex> lk(t.mu);
+  t.m[std::make_tuple(dev, (int)kind, (int)dim, (int)gradient)] = {layout, tile};
+  return ZEUS_OK;
+}
+
+int
+zeus_autotune(const zeus_problem* problem, const zeus_bfgs_config* config,
+              int64_t n_sample, uint64_t seed, double lower, double upper,
+              int32_t* best_layout, int32_t* best_tile, float* best_ms,
+              void* stream)
+{
+  int rc = check_problem(problem);
+  if (rc)
+    return rc;
+  if ((rc = check_config(config)))
+    return rc;
+  if (config->mode != ZEUS_MODE_FAST || n_sample <= 0) {
+    set_error("zeus_autotune: fast mode and n_sample > 0 required");
+    return ZEUS_E_INVALID;
+  }
+  const int kind = problem->kind, dim = problem->dim;
+  std::vector<std::pair<int, int>> cand;
+  if (thread_layout_supported(kind, dim))
+    cand.push_back({ZEUS_LAYOUT_THREAD, 0});
+  const unsigned w = tile_widths(kind, dim);
+  for (int k = 1; k <= 5; ++k)
+    if ((w >> k) & 1u)
+      cand.push_back({ZEUS_LAYOUT_TILE, 1 << k});
+  if (cta_layout_supported(kind, dim))
+    cand.push_back({ZEUS_LAYOUT_CTA, 0});
+  if (cand.empty()) {
+    set_error("zeus_autotune: no layout built for kind %d dim %d", kind, dim);
+    return ZEUS_E_UNSUPPORTED;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<void*> allocs;
+  auto cleanup = [&]() {
+    for (void* p : allocs)
+      cudaFreeAsync(p, st);
+    cudaStreamSynchronize(st);
+  };
+  auto alloc = [&](size_t bytes, void** out) -> int {
+    const int r = cuda_fail(cudaMallocAsync(out, bytes ? bytes : 1, st),
+                            "autotune allocation");
+    if (r == ZEUS_OK)
+      allocs.push_back(*out);
+    return r;
+  };
+  void *starts, *fval, *status, *iters, *gnorm, *xo, *ctl, *ws;
+  const size_t nd = (size_t)n_sample * dim;
+  zeus_bfgs_config c0 = *config;
+  c0.layout = ZEUS_LAYOUT_TILE; // any; the workspace does not depend on it
+  const size_t wsz = zeus_bfgs_workspace_size(problem, &c0, n_sample);
+  if ((rc = alloc(sizeof(double) * nd, &starts)) ||
+      (rc = alloc(sizeof(double) * n_sample, &fval)) ||
+      (rc = alloc(sizeof(int32_t) * n_sample, &status)) ||
+      (rc = alloc(sizeof(int32_t) * n_sample, &iters)) ||
+      (rc = alloc(sizeof(double) * n_sample, &gnorm)) ||
+      (rc = alloc(sizeof(double) * nd, &xo)) ||
+      (rc = alloc(sizeof(int32_t) * 2, &ctl)) || (rc = alloc(wsz, &ws))) {
+    cleanup();
+    return rc;
+  }
+  if ((rc = zeus_starts_uniform(seed, n_sample, dim, lower, upper,
+                                static_cast<double*>(starts), st))) {
+    cleanup();
+    return rc;
+  }
+  zeus_run_outputs ro{};
+  ro.fval = static_cast<double*>(fval);
+  ro.status = static_cast<int32_t*>(status);
+  ro.iter = static_cast<int32_t*>(iters);
+  ro.gnorm = static_cast<double*>(gnorm);
+  ro.x = static_cast<double*>(xo);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 3.4e38f;
+  int bl = -1, bt = 0;
+  for (auto [layout, tile] : cand) {
+    zeus_bfgs_config c = *config;
+    c.layout = layout;
+    c.tile = tile;
+    float ms_min = 3.4e38f;
+    for (int rep = 0; rep < 2 && rc == ZEUS_OK; ++rep) { // warm-up + timed
+      cudaMemsetAsync(ctl, 0, sizeof(int32_t) * 2, st);
+      cudaEventRecord(e0, st);
+      rc = zeus_bfgs_device(problem, &c, static_cast<double*>(starts), n_sample,
+                            &ro, static_cast<int32_t*>(ctl), ws, wsz, st);
+      cudaEventRecord(e1, st);
+      if (rc == ZEUS_OK)
+        rc = cuda_fail(cudaEventSynchronize(e1), "autotune run");
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0)
+        ms_min = ms;
+    }
+    if (rc != ZEUS_OK)
+      break;
+    if (ms_min < best) {
+      best = ms_min;
+      bl = layout;
+      bt = tile;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cleanup();
+  if (rc != ZEUS_OK)
+    return rc;
+  zeus_autotune_record(kind, dim, config->gradient, bl, bt);
+  if (best_layout)
+    *best_layout = bl;
+  if (best_tile)
+    *best_tile = bt;
+  if (best_ms)
+    *best_ms = best;
+  return ZEUS_OK;
 }
 
 void

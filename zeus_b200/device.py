@@ -11,7 +11,7 @@ from typing import Optional
 import numpy as np
 import torch
 
-from . import (BfgsConfig, Objective, RunOutputs, check, lib, make_config,
+from . import (BatchClass, BfgsConfig, Objective, RunOutputs, check, lib, make_config,
                LAYOUT_AUTO)
 
 
@@ -143,3 +143,83 @@ def census_device(fval: torch.Tensor, status: torch.Tensor, x: Optional[torch.Te
     v = out.cpu().tolist()
     return dict(actual=v[0], claimed=v[1], surrendered=v[2], stopped=v[3],
                 best_idx=v[4])
+
+
+class BatchJob:
+    """One class of a persistent batch: an objective (optionally with several
+    data instances stored one after another), its starts on the GPU and its
+    own outputs and stop-early control."""
+
+    def __init__(self, obj, starts: torch.Tensor, required: Optional[int] = None,
+                 layout: int = LAYOUT_AUTO, tile: int = 0, runs_per_instance: int = 0,
+                 counters: bool = True):
+        self.dp = obj if isinstance(obj, DeviceProblem) else DeviceProblem(obj, starts.device)
+        if starts.dtype != torch.float64 or not starts.is_cuda or not starts.is_contiguous():
+            raise ValueError("starts must be a contiguous float64 CUDA tensor")
+        self.starts = starts
+        self.n = starts.shape[0]
+        self.required = self.n + 1 if required is None else required
+        self.layout, self.tile, self.rpi = layout, tile, runs_per_instance
+        dev = starts.device
+        dim = self.dp.obj.dim
+        self.fval = torch.empty((self.n,), dtype=torch.float64, device=dev)
+        self.status = torch.empty((self.n,), dtype=torch.int32, device=dev)
+        self.iter = torch.empty((self.n,), dtype=torch.int32, device=dev)
+        self.gnorm = torch.empty((self.n,), dtype=torch.float64, device=dev)
+        self.x = torch.empty((self.n, dim), dtype=torch.float64, device=dev)
+        self.counters = (torch.zeros((self.n, 3), dtype=torch.int64, device=dev)
+                         if counters else None)
+        self.control = torch.zeros((2,), dtype=torch.int32, device=dev)
+
+    def c(self) -> BatchClass:
+        out = RunOutputs(_ptr(self.fval), _ptr(self.status), _ptr(self.iter),
+                         _ptr(self.gnorm), _ptr(self.x), _ptr(self.counters),
+                         None, None, None, None)
+        prob = self.dp.c()
+        if self.rpi and self.dp.idata is not None:
+            # ndata is per instance
+            ninst = (self.n + self.rpi - 1) // self.rpi
+            prob.ndata = self.dp.idata.numel() // ninst
+        return BatchClass(prob, self.n, self.rpi, _ptr(self.starts), out,
+                          _ptr(self.control), self.required, self.layout, self.tile, 0)
+
+
+class Batch:
+    """A persistent-batch launch with preallocated workspace."""
+
+    def __init__(self, jobs, max_iter: int = 10000, tol: float = 1e-8, flags: int = 0):
+        self.jobs = list(jobs)
+        self.cfg = make_config(max_iter, 1, tol, "fast", "adjoint", flags=flags)
+        self.arr = (BatchClass * len(self.jobs))(*[j.c() for j in self.jobs])
+        self.wsz = lib().zeus_batch_workspace_size(self.arr, len(self.jobs))
+        dev = self.jobs[0].starts.device
+        self.ws = torch.empty((max(self.wsz, 1),), dtype=torch.uint8, device=dev)
+
+    def launch(self, stream=None, reset=True):
+        if reset:
+            for j in self.jobs:
+                j.control.zero_()
+        check(lib().zeus_batch_device(self.arr, len(self.jobs), C.byref(self.cfg),
+                                      _ptr(self.ws), self.wsz, _stream_handle(stream)))
+        return self
+
+
+def batch_device(jobs, max_iter: int = 10000, tol: float = 1e-8, flags: int = 0,
+                 stream=None) -> Batch:
+    """Runs every BatchJob in one persistent kernel launch."""
+    return Batch(jobs, max_iter, tol, flags).launch(stream)
+
+
+def autotune(obj, n_sample: int = 2048, max_iter: int = 10000, tol: float = 1e-8,
+             lower: float = -5.0, upper: float = 5.0, seed: int = 1,
+             gradient: str = "adjoint", device="cuda", stream=None):
+    """Times every built layout for `obj` and records the fastest; returns
+    (layout, tile, ms)."""
+    dp = _as_problem(obj, device)
+    cfg = make_config(max_iter, n_sample + 1, tol, "fast", gradient)
+    lay, til, ms = C.c_int32(), C.c_int32(), C.c_float()
+    prob = dp.c()
+    check(lib().zeus_autotune(C.byref(prob), C.byref(cfg), n_sample, seed, lower, upper,
+                              C.byref(lay), C.byref(til), C.byref(ms),
+                              _stream_handle(stream)))
+    return lay.value, til.value, ms.value
