@@ -275,6 +275,10 @@ def run_gpu(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     wl = workloads()[args.workload]
     jobs = wl["jobs"]
+    if args.scale != 1.0:
+        for j in jobs:
+            per = j.runs_per_instance or 1
+            j.n = max(per, int(round(j.n * args.scale / per)) * per)
     dev = torch.device("cuda", local_rank)
     # a dedicated (non-legacy) stream: the PSO loop is captured into a CUDA
     # graph on it
@@ -715,6 +719,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the plain dual-AD comparison")
     ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="multiply every class's run count (small cases for profiling)")
     ap.add_argument("--write-iterations", default="",
                     help="write per-class iteration statistics (for the reference arm)")
     args = ap.parse_args()

@@ -1,0 +1,450 @@
+// zeus.cuh -- C++ drop-in for the reference's public API on B200 (sm_100a).
+//
+//   #include "zeus.cuh"       (nvcc -std=c++20 --expt-relaxed-constexpr
+//                              -I include -I zeus_b200/csrc, link
+//                              zeus_b200/libzeus_b200.so)
+//   auto r = zeus::Zeus(f, lower, upper, N, MAX_ITER, PSO_ITER,
+//                       requiredConverged, "name", tol, seed, run);
+//
+// Keeps the reference's call surface (include/zeus.cuh:341-375): the
+// callable f is any functor with `template <class T> __host__ __device__ T
+// operator()(std::array<T, D> const&) const`, its dimension D comes from
+// zeus::FnTraits (static `arity`, or a Functor<D> template), it is validated
+// by the ZeusObjective concept, objective data lives in Matrix<T> members
+// read through .data(), and the result is zeus::Result<D> with the
+// reference's field names and status codes (util.hpp:16-54).
+//
+// The kernels that evaluate f are templates instantiated here, in the
+// caller's translation unit, from the library's own headers (PSO:
+// zb_pso.cuh; BFGS layouts: zb_bfgs_thread.cuh / zb_bfgs_coop.cuh); the
+// objective-independent work (argmin and status census) goes through the
+// C ABI in zeus_b200.h.  Gradients are D forward dual passes unless the
+// functor also has `double adjoint(const double* x, double* g) const`
+// (hand-written gradient), which is then used.  Layout by dimension:
+// thread-per-run (D <= 8), 32-lane tile (D <= 32), block-per-run with H in
+// shared memory (up to D = 160).
+#pragma once
+
+#include <array>
+#include <cstddef>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <string_view>
+#include <type_traits>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "zeus_b200.h"
+#include "zb_bfgs_coop.cuh"
+#include "zb_bfgs_thread.cuh"
+#include "zb_dual.cuh"
+#include "zb_pso.cuh"
+
+namespace zeus {
+
+  // ---- traits (the reference's traits.hpp:19-71) --------------------------
+  template <typename...>
+  using VoidT = void;
+
+  template <typename F, typename = void>
+  struct FnTraits {
+    static constexpr std::size_t arity = 0;
+  };
+  template <typename F>
+  struct FnTraits<F, VoidT<decltype(F::arity)>> {
+    static constexpr std::size_t arity = F::arity;
+  };
+  template <template <std::size_t> class Functor, std::size_t N>
+  struct FnTraits<Functor<N>> {
+    static constexpr std::size_t arity = N;
+  };
+
+  template <typename F, typename T, std::size_t DIM>
+  concept CallableWithArray = requires(F f, std::array<T, DIM> arr) {
+    { f(arr) } -> std::convertible_to<T>;
+  };
+  template <typename F, std::size_t DIM>
+  concept ZeusObjective = CallableWithArray<F, double, DIM> &&
+                          CallableWithArray<F, dual::DualNumber, DIM>;
+
+  enum class PRNGType { XORWOW, PHILOX, SOBOL };
+
+  // ---- results (util.hpp:16-54) -------------------------------------------
+  struct Metrics {
+    const char* label = "";
+    double ms_per_call = 0.0;
+    double calls_per_thread_mean = 0.0;
+    double fraction_of_kernel = 0.0;
+    double block95 = 0.0;
+    double serialized = 0.0;
+    double fraction_of_thread = 0.0;
+  };
+  struct Convergence {
+    int actual = 0;
+    int claimed = 0;
+    int surrendered = 0;
+    int stopped = 0;
+  };
+  template <std::size_t DIM>
+  struct Result {
+    int idx = -1;
+    int status = -1; // 0 surrender, 1 converged, 2 stopped, 3 alloc, 4 CUDA, 5 non-finite
+    double fval = 37.0;
+    double gradientNorm = 0.0;
+    double coordinates[DIM]{};
+    int iter = 0;
+    Convergence c;
+    double ms_opt = 0.0;
+    Metrics ad;
+    Metrics bfgs;
+  };
+
+} // namespace zeus
+
+// ---- objective data (the reference's matrix.hpp:20-258) --------------------
+// Host and device copies of a dense rows x cols matrix.  data() returns the
+// device pointer in device code and the host pointer in host code.  Copies
+// share the buffers (reference-counted on the host), so an objective holding
+// a Matrix is cheap to copy into kernel parameters; set(...) writes the host
+// copy and pushes it to the device, syncHost2Device() pushes the whole host
+// copy after direct edits through operator() / hostData().
+template <typename T>
+class Matrix {
+  struct Block {
+    T* host = nullptr;
+    T* device = nullptr;
+    ~Block()
+    {
+      std::free(host);
+      if (device)
+        cudaFree(device);
+    }
+  };
+  T* host_data_ = nullptr;
+  T* device_data_ = nullptr;
+  std::size_t rows_ = 0, cols_ = 0;
+  std::shared_ptr<Block>* owner_ = nullptr; // host-side share count
+
+  static void
+  check(cudaError_t e)
+  {
+    if (e != cudaSuccess)
+      throw std::runtime_error(std::string("CUDA error: ") + cudaGetErrorString(e));
+  }
+  void
+  bounds(std::size_t i, std::size_t j) const
+  {
+    if (i >= rows_ || j >= cols_)
+      throw std::out_of_range("Matrix index out of range");
+  }
+  void
+  release()
+  {
+    delete owner_;
+    owner_ = nullptr;
+    host_data_ = device_data_ = nullptr;
+  }
+
+public:
+  Matrix() noexcept = default;
+  Matrix(std::size_t rows, std::size_t cols) : rows_(rows), cols_(cols)
+  {
+    if (!rows || !cols)
+      throw std::invalid_argument("Matrix dimensions must be > 0");
+    auto b = std::make_shared<Block>();
+    b->host = static_cast<T*>(std::calloc(rows * cols, sizeof(T)));
+    if (!b->host)
+      throw std::runtime_error("host malloc failed");
+    check(cudaMalloc(&b->device, rows * cols * sizeof(T)));
+    host_data_ = b->host;
+    device_data_ = b->device;
+    owner_ = new std::shared_ptr<Block>(std::move(b));
+  }
+  template <std::size_t N>
+  Matrix(std::size_t rows, std::size_t cols, const std::array<T, N>& init)
+    : Matrix(rows, cols)
+  {
+    set(init);
+  }
+  __host__ __device__ Matrix(const Matrix& o)
+    : host_data_(o.host_data_), device_data_(o.device_data_), rows_(o.rows_),
+      cols_(o.cols_)
+  {
+#ifndef __CUDA_ARCH__
+    owner_ = o.owner_ ? new std::shared_ptr<Block>(*o.owner_) : nullptr;
+#endif
+  }
+  Matrix&
+  operator=(const Matrix& o)
+  {
+    if (this != &o) {
+      release();
+      host_data_ = o.host_data_;
+      device_data_ = o.device_data_;
+      rows_ = o.rows_;
+      cols_ = o.cols_;
+      owner_ = o.owner_ ? new std::shared_ptr<Block>(*o.owner_) : nullptr;
+    }
+    return *this;
+  }
+  __host__ __device__ ~Matrix()
+  {
+#ifndef __CUDA_ARCH__
+    release();
+#endif
+  }
+
+  void
+  set(std::size_t i, std::size_t j, const T& x)
+  {
+    bounds(i, j);
+    host_data_[i * cols_ + j] = x;
+    check(cudaMemcpy(device_data_ + i * cols_ + j, &x, sizeof(T),
+                     cudaMemcpyHostToDevice));
+  }
+  template <std::size_t N>
+  void
+  set(const std::array<T, N>& a)
+  {
+    set(a.data(), N);
+  }
+  void
+  set(const T* host_ptr, std::size_t count)
+  {
+    if (count != rows_ * cols_)
+      throw std::invalid_argument("count must equal rows*cols");
+    std::memcpy(host_data_, host_ptr, count * sizeof(T));
+    syncHost2Device();
+  }
+  void
+  syncHost2Device()
+  {
+    check(cudaMemcpy(device_data_, host_data_, rows_ * cols_ * sizeof(T),
+                     cudaMemcpyHostToDevice));
+  }
+  __host__ __device__ const T*
+  data() const noexcept
+  {
+#ifdef __CUDA_ARCH__
+    return device_data_;
+#else
+    return host_data_;
+#endif
+  }
+  T*
+  hostData() noexcept
+  {
+    return host_data_;
+  }
+  const T*
+  hostData() const noexcept
+  {
+    return host_data_;
+  }
+  T*
+  deviceData() noexcept
+  {
+    return device_data_;
+  }
+  const T*
+  deviceData() const noexcept
+  {
+    return device_data_;
+  }
+  T&
+  operator()(std::size_t i, std::size_t j)
+  {
+    bounds(i, j);
+    return host_data_[i * cols_ + j];
+  }
+  const T&
+  operator()(std::size_t i, std::size_t j) const
+  {
+    bounds(i, j);
+    return host_data_[i * cols_ + j];
+  }
+  std::size_t
+  rows() const noexcept
+  {
+    return rows_;
+  }
+  std::size_t
+  cols() const noexcept
+  {
+    return cols_;
+  }
+};
+
+namespace zeus {
+
+  namespace detail {
+
+    struct DeviceBuffers {
+      std::vector<void*> p;
+      cudaStream_t st = nullptr;
+      ~DeviceBuffers()
+      {
+        for (void* q : p)
+          cudaFreeAsync(q, st);
+        cudaStreamSynchronize(st);
+      }
+      template <class T>
+      T*
+      alloc(std::size_t n)
+      {
+        void* q = nullptr;
+        const cudaError_t e = cudaMallocAsync(&q, n ? n * sizeof(T) : 1, st);
+        if (e != cudaSuccess)
+          throw e;
+        p.push_back(q);
+        return static_cast<T*>(q);
+      }
+    };
+
+    template <class F, std::size_t D>
+    cudaError_t
+    launch_bfgs(const F& f, const zb::BfgsParams& prm, const double* starts,
+                const zb::RunOut& out, zb::Control* ctl, cudaStream_t st)
+    {
+      constexpr bool kAdj = zb::HasAdjoint<F>;
+      if constexpr (D <= 8) {
+        const unsigned grid = (unsigned)((prm.n + 127) / 128);
+        zb::bfgs_thread_kernel<F, (int)D, kAdj>
+          <<<grid, 128, 0, st>>>(f, prm, starts, out, ctl);
+      } else if constexpr (D <= 32) {
+        constexpr int TS = 32, TPB = zb::kTileBlock / TS;
+        const unsigned grid = (unsigned)((prm.n + TPB - 1) / TPB);
+        const size_t smem =
+          sizeof(double) * TPB * zb::tile_smem_doubles<(int)D, TS>();
+        zb::bfgs_tile_kernel<F, (int)D, TS, kAdj>
+          <<<grid, zb::kTileBlock, smem, st>>>(f, prm, starts, out, ctl);
+      } else {
+        static_assert(D <= 160, "dimensions above 160 are not supported");
+        constexpr int B = D <= 64 ? 256 : 512;
+        const size_t smem = sizeof(double) * zb::cta_smem_doubles<(int)D>(B);
+        auto k = zb::bfgs_cta_kernel<F, (int)D, kAdj, B>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, B, smem);
+        const int64_t cap = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
+        k<<<(unsigned)(prm.n < cap ? prm.n : cap), B, smem, st>>>(f, prm, starts,
+                                                                  out, ctl);
+      }
+      return cudaGetLastError();
+    }
+
+  } // namespace detail
+
+  // The reference's entry point (include/zeus.cuh:341-375).  parallel,
+  // prng_type and nzerosteps are accepted for source compatibility: the
+  // layout follows the dimension, starts and PSO draws come from Philox, and
+  // the zero-step limit cannot trigger (the reference's line search never
+  // returns 0, utils.cuh:395-411).  trajectory_file is not written.
+  template <typename Function, std::size_t ZEUS_DIM = FnTraits<Function>::arity>
+    requires ZeusObjective<Function, ZEUS_DIM>
+  Result<ZEUS_DIM>
+  Zeus(Function const& f, double lower, double upper, std::size_t N,
+       int MAX_ITER, int PSO_ITER, int requiredConverged,
+       std::string_view fun_name, double tolerance, int seed, int run,
+       bool parallel = true, PRNGType prng_type = PRNGType::XORWOW,
+       std::string_view trajectory_file = {}, int nzerosteps = 0)
+  {
+    (void)parallel;
+    (void)prng_type;
+    (void)trajectory_file;
+    (void)nzerosteps;
+    (void)run;
+    constexpr std::size_t D = ZEUS_DIM;
+    Result<D> best;
+    if (N == 0)
+      return best; // zeus.cuh:58-60
+    detail::DeviceBuffers b;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    try {
+      const int64_t n = (int64_t)N;
+      double* starts = b.alloc<double>(N * D);
+      double* fval = b.alloc<double>(N);
+      int32_t* status = b.alloc<int32_t>(N);
+      int32_t* iter = b.alloc<int32_t>(N);
+      double* gnorm = b.alloc<double>(N);
+      double* x = b.alloc<double>(N * D);
+      int32_t* ctl = b.alloc<int32_t>(2);
+      zeus_census* cen = b.alloc<zeus_census>(1);
+      cudaMemsetAsync(ctl, 0, 2 * sizeof(int32_t), b.st);
+      if (PSO_ITER >= 0) {
+        const int64_t blocks = (n + zb::kPsoBlock - 1) / zb::kPsoBlock;
+        zb::PsoWork w;
+        w.X = b.alloc<double>(N * D);
+        w.V = b.alloc<double>(N * D);
+        w.part_key = b.alloc<unsigned long long>(blocks);
+        w.part_idx = b.alloc<int>(blocks);
+        w.counter = b.alloc<unsigned int>(1);
+        w.gbest = b.alloc<double>(D + 1);
+        double* pbf = b.alloc<double>(N);
+        zb::pso_reset_kernel<(int)D><<<1, 256, 0, b.st>>>(w);
+        zb::pso_init_kernel<Function, (int)D>
+          <<<(unsigned)blocks, zb::kPsoBlock, 0, b.st>>>(f, n, lower, upper,
+                                                         (uint64_t)seed, w,
+                                                         starts, pbf);
+        for (int t = 1; t <= PSO_ITER; ++t)
+          zb::pso_iter_kernel<Function, (int)D>
+            <<<(unsigned)blocks, zb::kPsoBlock, 0, b.st>>>(
+              f, n, 0.5, 1.2, 1.5, (uint64_t)seed, t, w, starts, pbf);
+      } else if (zeus_starts_uniform((uint64_t)seed, n, (int32_t)D, lower, upper,
+                                     starts, b.st) != ZEUS_OK) {
+        throw cudaErrorLaunchFailure;
+      }
+      zb::BfgsParams prm{n, MAX_ITER, requiredConverged, tolerance, 0};
+      zb::RunOut out{fval,   status,  iter,    gnorm,   x,
+                     nullptr, nullptr, nullptr, nullptr, nullptr};
+      cudaEventRecord(e0, b.st);
+      cudaError_t e = detail::launch_bfgs<Function, D>(
+        f, prm, starts, out, reinterpret_cast<zb::Control*>(ctl), b.st);
+      cudaEventRecord(e1, b.st);
+      if (e != cudaSuccess)
+        throw e;
+      std::vector<double> km;
+      if (fun_name == "rosenbrock")
+        km.assign(D, 1.0);
+      if (zeus_census_device(fval, status, x, n, (int32_t)D,
+                             km.empty() ? nullptr : km.data(), cen, b.st) != ZEUS_OK)
+        throw cudaErrorLaunchFailure;
+      zeus_census hc{};
+      cudaMemcpyAsync(&hc, cen, sizeof hc, cudaMemcpyDeviceToHost, b.st);
+      if ((e = cudaStreamSynchronize(b.st)) != cudaSuccess)
+        throw e;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      best.ms_opt = ms;
+      best.c = Convergence{hc.actual, hc.claimed, hc.surrendered, hc.stopped};
+      if (hc.best_idx >= 0) {
+        const int i = hc.best_idx;
+        cudaMemcpy(&best.fval, fval + i, sizeof(double), cudaMemcpyDeviceToHost);
+        cudaMemcpy(&best.status, status + i, sizeof(int), cudaMemcpyDeviceToHost);
+        cudaMemcpy(&best.iter, iter + i, sizeof(int), cudaMemcpyDeviceToHost);
+        cudaMemcpy(&best.gradientNorm, gnorm + i, sizeof(double),
+                   cudaMemcpyDeviceToHost);
+        cudaMemcpy(best.coordinates, x + (size_t)i * D, sizeof(double) * D,
+                   cudaMemcpyDeviceToHost);
+        best.idx = i;
+      }
+    } catch (cudaError_t e) { // zeus.cuh:112-116: 3 allocation, 4 runtime
+      best = Result<D>{};
+      best.status = (e == cudaErrorMemoryAllocation) ? 3 : 4;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
+  }
+
+} // namespace zeus

@@ -106,9 +106,9 @@ def test_batch_rejects_bad_input(cuda):
     st = starts_uniform(1, 8, 3, -1.0, 1.0)
     with pytest.raises(zb.ZeusError):
         batch_device([BatchJob(zb.Objective(ROS, 3), st)])
-    st = starts_uniform(1, 8, 8, -1.0, 1.0)
+    st = starts_uniform(1, 8, 32, -1.0, 1.0)  # 16 H rows of 32 per lane: not built
     with pytest.raises(zb.ZeusError):
-        batch_device([BatchJob(zb.Rosenbrock(8), st, layout=zb.LAYOUT_TILE, tile=2)])
+        batch_device([BatchJob(zb.Rosenbrock(32), st, layout=zb.LAYOUT_TILE, tile=2)])
 
 
 @pytest.mark.parametrize("obj,lo,hi", [(zb.Rosenbrock(8), -5, 5), (zb.Rastrigin(10), -5.12, 5.12),

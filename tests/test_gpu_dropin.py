@@ -1,0 +1,58 @@
+"""The C++ drop-in (include/zeus.cuh: zeus::Zeus, Matrix, Result) used as code
+written for the reference uses it: tests/cpp/dropin_test.cu, built by
+zeus_b200/build.py into zeus_b200/_bin/dropin_test."""
+import json
+import subprocess
+
+import numpy as np
+import pytest
+
+from zeus_b200 import build as zbuild
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def results(cuda):
+    exe = zbuild.DROPIN_BIN
+    if not exe.exists():
+        pytest.fail(f"{exe} is missing: run zeus_b200/build.py (build_dropin_test)")
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    return {d["case"]: d for d in (json.loads(l) for l in out.stdout.splitlines()
+                                   if l.startswith("{"))}
+
+
+def test_rosenbrock_functor(results):
+    r = results["rosenbrock"]
+    assert r["status"] in (1, 2) and r["fval"] < 1e-12
+    np.testing.assert_allclose(r["x"], [1.0, 1.0], atol=1e-6)
+    assert r["claimed"] >= 100 and r["claimed"] + r["stopped"] + r["surrendered"] == 1024
+
+
+def test_functor_template_dimension_and_tile_layout(results):
+    r = results["sphere16"]
+    assert r["status"] == 1 and r["gnorm"] < 1e-8
+    np.testing.assert_allclose(r["x"], [0.5] * 16, atol=1e-8)
+
+
+def test_matrix_backed_objective(results):
+    r = results["gaussian8"]
+    assert r["status"] == 1 and abs(r["fval"]) < 1e-15
+    np.testing.assert_allclose(r["x"], [0.0] * 8, atol=1e-8)
+
+
+def test_adjoint_member_and_uniform_starts(results):
+    r = results["adjoint4"]
+    assert r["status"] == 1 and r["fval"] < 1e-16
+
+
+def test_cta_layout_from_template(results):
+    r = results["sphere40"]
+    assert r["status"] == 1
+    np.testing.assert_allclose(r["x"], [0.5] * 40, atol=1e-8)
+
+
+def test_zero_runs_default_result(results):
+    r = results["empty"]
+    assert r["status"] == -1 and r["fval"] == 37.0 and r["idx"] == -1

@@ -89,5 +89,28 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
     return LIB
 
 
+BIN = HERE / "_bin"
+DROPIN_SRC = ROOT / "tests" / "cpp" / "dropin_test.cu"
+DROPIN_BIN = BIN / "dropin_test"
+
+
+def build_dropin_test(verbose: bool = False) -> Path:
+    """Compiles the C++ drop-in test program against libzeus_b200.so."""
+    lib = build(verbose)
+    BIN.mkdir(exist_ok=True)
+    deps = [DROPIN_SRC, INCLUDE / "zeus.cuh", lib] + list(CSRC.glob("*.cuh"))
+    if DROPIN_BIN.exists() and DROPIN_BIN.stat().st_mtime >= max(
+            d.stat().st_mtime for d in deps):
+        return DROPIN_BIN
+    cmd = [nvcc(), *COMMON, str(DROPIN_SRC), "-o", str(DROPIN_BIN), "-L", str(HERE),
+           "-lzeus_b200", "-Xlinker", "-rpath,$ORIGIN/.."]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"drop-in test build failed:\n{r.stdout}\n{r.stderr}")
+    return DROPIN_BIN
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))

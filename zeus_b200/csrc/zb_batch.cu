@@ -198,7 +198,7 @@ namespace zb {
     cta_doubles_rt(int d, int block)
     {
       const int q = block >= d ? block / d : 1;
-      return (size_t)d * d + 11 * d + 2 * q * d + 32 * 8 + block + 4;
+      return (size_t)d * d + 11 * d + 2 * q * d + 32 * 8 + block + 8 + 4;
     }
 
     bool

@@ -328,13 +328,29 @@ namespace zb {
 
   // ---------------------------------------------------------------- CTA
   // Shared-memory layout (doubles): H[D*D] | 11 vectors of D | partial sums
-  // 2*Q*D | reduction 32*8 | scratch blockDim | flags (as doubles) 4.
+  // 2*Q*D (also the line-search trial points) | reduction 32*8 | scratch
+  // blockDim | trial values 8 | flags 4.
   template <int D>
   __host__ __device__ constexpr size_t
   cta_smem_doubles(int block)
   {
     const int q = block >= D ? block / D : 1;
-    return (size_t)D * D + 11 * D + 2 * q * D + 32 * 8 + block + 4;
+    return (size_t)D * D + 11 * D + 2 * q * D + 32 * 8 + block + 8 + 4;
+  }
+
+  // Line-search trials evaluated at once in the CTA layout: the block splits
+  // into groups of round32(D) threads, one trial point each; none when the
+  // trials carry a gradient (the Gaussian's C x needs the whole block).
+  template <class F, int D, bool Adjoint, int kBlock>
+  __host__ __device__ constexpr int
+  cta_trials_per_round()
+  {
+    constexpr int dr = (D + 31) / 32 * 32;
+    constexpr int k = kBlock / dr;
+    if constexpr (Adjoint && TrialsWithGradient<F>)
+      return 1;
+    else
+      return k < 1 ? 1 : (k > 8 ? 8 : k);
   }
 
   // One run on the whole block (blockDim.x == kBlock): `sm` holds
@@ -346,6 +362,10 @@ namespace zb {
           Control* ctl)
   {
     constexpr int Q = kBlock >= D ? kBlock / D : 1;
+    constexpr bool kTrialGrad = Adjoint && TrialsWithGradient<F>;
+    constexpr int DR = (D + 31) / 32 * 32;
+    constexpr int KT = cta_trials_per_round<F, D, Adjoint, kBlock>();
+    static_assert(KT <= Q, "trial points reuse the partial-sum area");
     double* H = sm;
     double* x = H + D * D;
     double* g = x + D;
@@ -362,46 +382,83 @@ namespace zb {
     double* partH = partU + Q * D;
     double* red = partH + Q * D;
     double* scratch = red + 32 * 8;
-    int* flags = reinterpret_cast<int*>(scratch + kBlock);
+    double* trial_f = scratch + kBlock;
     CtaGroup grp{red, scratch};
     const int t = threadIdx.x;
-    constexpr bool kTrialGrad = Adjoint && TrialsWithGradient<F>;
 
+    for (int i = t; i < D; i += kBlock)
+      x[i] = x0[i];
+    for (int e = t; e < D * D; e += kBlock)
+      H[e] = (e / D == e % D) ? 1.0 : 0.0;
+    __syncthreads();
+    double best;
+    if constexpr (kTrialGrad)
+      best = coop_gradient<F, D, Adjoint>(f, grp, x, g);
+    else {
+      best = coop_value<F, D>(f, grp, x);
+      coop_gradient<F, D, Adjoint>(f, grp, x, g);
+    }
+    __syncthreads();
+    double ddir;
+    bool stop;
     {
-      for (int i = t; i < D; i += kBlock)
-        x[i] = x0[i];
-      for (int e = t; e < D * D; e += kBlock)
-        H[e] = (e / D == e % D) ? 1.0 : 0.0;
-      __syncthreads();
-      double best;
-      if constexpr (kTrialGrad)
-        best = coop_gradient<F, D, Adjoint>(f, grp, x, g);
-      else {
-        best = coop_value<F, D>(f, grp, x);
-        coop_gradient<F, D, Adjoint>(f, grp, x, g);
-      }
-      __syncthreads();
-      for (int i = t; i < D; i += kBlock)
+      double v[2] = {0.0, t == 0 ? (double)load_stop(ctl) : 0.0};
+      for (int i = t; i < D; i += kBlock) {
         p[i] = -g[i];
-      long long n_eval = 1, n_grad = 1;
-      int status = kUnset, iter, executed = -1;
-      double fout = best, gout = 0.0;
-      __syncthreads();
+        v[0] = fma(g[i], p[i], v[0]);
+      }
+      grp.template sum<2>(v);
+      ddir = v[0];
+      stop = v[1] != 0.0;
+    }
+    long long n_eval = 1, n_grad = 1;
+    int status = kUnset, iter, executed = -1;
+    double fout = best, gout = 0.0;
 
-      for (iter = 0; iter < prm.max_iter; ++iter) {
-        if (t == 0)
-          flags[0] = load_stop(ctl);
-        __syncthreads();
-        if (flags[0]) {
-          status = kStopped;
-          break;
+    for (iter = 0; iter < prm.max_iter; ++iter) {
+      if (stop) {
+        status = kStopped;
+        break;
+      }
+      // ---- line search: alpha_k = 2^-k, first k in 0..19 that passes,
+      // else alpha = 2^-20 (utils.cuh:376-412)
+      double fnew = 0.0;
+      bool have_grad = false;
+      if constexpr (KT > 1) {
+        const int q = t / DR, j = t % DR;
+        const bool inq = q < KT;
+        double* tx = partU + (inq ? q : 0) * D;
+        int found = -1;
+        double alpha = 0.0;
+        for (int r0 = 0; found < 0; r0 += KT) {
+          const int k = r0 + q;
+          if (inq && j < D && k <= kLineSearchTrials)
+            tx[j] = fma(ldexp(1.0, -k), p[j], x[j]);
+          __syncthreads();
+          const CtaSubGroup sg{red, scratch, DR};
+          const double f1 = coop_value<F, D>(f, sg, tx);
+          if (inq && j == 0)
+            trial_f[q] = f1;
+          __syncthreads();
+          for (int qq = 0; qq < KT; ++qq) {
+            const int kk = r0 + qq;
+            if (kk > kLineSearchTrials)
+              break;
+            const double fk = trial_f[qq], ak = ldexp(1.0, -kk);
+            if (kk == kLineSearchTrials ||
+                (fk <= best + kArmijoC1 * ak * ddir && fk < best)) {
+              found = kk;
+              fnew = fk;
+              alpha = ak;
+              break;
+            }
+          }
         }
-        double dd = 0.0;
+        n_eval += found + 1;
         for (int i = t; i < D; i += kBlock)
-          dd = fma(g[i], p[i], dd);
-        const double ddir = grp.sum(dd);
-        double alpha = 1.0, fnew = 0.0;
-        bool have_grad = false;
+          xn[i] = fma(alpha, p[i], x[i]);
+      } else {
+        double alpha = 1.0;
         for (int k = 0; k <= kLineSearchTrials; ++k) {
           for (int i = t; i < D; i += kBlock)
             xn[i] = fma(alpha, p[i], x[i]);
@@ -412,12 +469,8 @@ namespace zb {
           else
             f1 = coop_value<F, D>(f, grp, xn);
           ++n_eval;
-          if (k == kLineSearchTrials) {
-            fnew = f1;
-            have_grad = kTrialGrad;
-            break;
-          }
-          if (f1 <= best + kArmijoC1 * alpha * ddir && f1 < best) {
+          if (k == kLineSearchTrials ||
+              (f1 <= best + kArmijoC1 * alpha * ddir && f1 < best)) {
             fnew = f1;
             have_grad = kTrialGrad;
             break;
@@ -425,139 +478,143 @@ namespace zb {
           alpha *= 0.5;
           __syncthreads(); // xn fully read before the next trial writes it
         }
-        __syncthreads();
-        if (have_grad) {
-          for (int i = t; i < D; i += kBlock)
-            gn[i] = gt[i];
-        } else {
-          coop_gradient<F, D, Adjoint>(f, grp, xn, gn);
-          ++n_grad;
-        }
-        __syncthreads();
-        if (have_grad)
-          ++n_grad;
-        const bool take = fnew < best;
-        double sy_part = 0.0;
-        for (int i = t; i < D; i += kBlock) {
-          s[i] = xn[i] - x[i];
-          y[i] = gn[i] - g[i];
-          sy_part = fma(s[i], y[i], sy_part);
-        }
-        const double sy = grp.sum(sy_part); // (its barriers publish s, y)
-        const bool skipped = fabs(sy) < kMinCurvature;
-        const double* gnext = take ? gn : g;
-        // sweep 1: u = H y (if updating) and h = H g_next, by columns
-        {
-          const int i = t % D, q = t / D;
-          if (q < Q && t < Q * D) {
-            double au = 0.0, ah = 0.0;
-            for (int m = q; m < D; m += Q) {
-              const double hv = H[m * D + i];
-              ah = fma(hv, gnext[m], ah);
-              if (!skipped)
-                au = fma(hv, y[m], au);
-            }
-            partU[q * D + i] = au;
-            partH[q * D + i] = ah;
-          }
-        }
-        __syncthreads();
-        double yu_part = 0.0;
-        for (int i = t; i < D; i += kBlock) {
+      }
+      __syncthreads();
+      if (have_grad) {
+        for (int i = t; i < D; i += kBlock)
+          gn[i] = gt[i];
+      } else {
+        coop_gradient<F, D, Adjoint>(f, grp, xn, gn);
+      }
+      ++n_grad;
+      __syncthreads();
+      const bool take = fnew < best;
+      double sy_part = 0.0;
+      for (int i = t; i < D; i += kBlock) {
+        s[i] = xn[i] - x[i];
+        y[i] = gn[i] - g[i];
+        sy_part = fma(s[i], y[i], sy_part);
+      }
+      const double sy = grp.sum(sy_part); // (its barriers publish s, y)
+      const bool skipped = fabs(sy) < kMinCurvature;
+      const double* gnext = take ? gn : g;
+      // sweep 1: u = H y (if updating) and h = H g_next, by columns
+      {
+        const int i = t % D, q = t / D;
+        if (q < Q && t < Q * D) {
           double au = 0.0, ah = 0.0;
-          for (int q = 0; q < Q; ++q) {
-            au += partU[q * D + i];
-            ah += partH[q * D + i];
+          for (int m = q; m < D; m += Q) {
+            const double hv = H[m * D + i];
+            ah = fma(hv, gnext[m], ah);
+            if (!skipped)
+              au = fma(hv, y[m], au);
           }
-          u[i] = au;
-          h[i] = ah;
-          yu_part = fma(y[i], au, yu_part);
-        }
-        if (!skipped) {
-          const double yu = grp.sum(yu_part);
-          const double rho = 1.0 / sy;
-          const double hb = 0.5 * rho * fma(rho, yu, 1.0);
-          double wg = 0.0, sg = 0.0;
-          for (int i = t; i < D; i += kBlock) {
-            const double wi = fma(hb, s[i], -rho * u[i]);
-            w[i] = wi;
-            wg = fma(wi, gnext[i], wg);
-            sg = fma(s[i], gnext[i], sg);
-          }
-          double v[2] = {wg, sg};
-          grp.template sum<2>(v); // barriers publish w
-          // sweep 2: H += s w^T + w s^T
-          for (int e = t; e < D * D; e += kBlock) {
-            const int i = e / D, j = e - (e / D) * D;
-            H[e] += __dadd_rn(__dmul_rn(s[i], w[j]), __dmul_rn(w[i], s[j]));
-          }
-          for (int i = t; i < D; i += kBlock)
-            p[i] = -(h[i] + s[i] * v[0] + w[i] * v[1]);
-        } else {
-          for (int i = t; i < D; i += kBlock)
-            p[i] = -h[i];
-        }
-        if (take) {
-          best = fnew;
-          for (int i = t; i < D; i += kBlock) {
-            x[i] = xn[i];
-            g[i] = gn[i];
-          }
-        }
-        __syncthreads();
-        double gg = 0.0;
-        for (int i = t; i < D; i += kBlock)
-          gg = fma(g[i], g[i], gg);
-        const double gnrm = sqrt(grp.sum(gg));
-        if (!isfinite(gnrm) || !isfinite(fnew)) {
-          status = kNonFinite;
-          fout = fnew;
-          gout = gnrm;
-          break;
-        }
-        if (gnrm < prm.tol) {
-          if (t == 0)
-            note_converged(ctl, prm.required);
-          status = kConverged;
-          fout = best;
-          gout = gnrm;
-          break;
-        }
-        if (!take && skipped && !(prm.flags & kFlagNoFixedPoint)) {
-          executed = iter + 1;
-          iter = prm.max_iter;
-          break;
-        }
-      }
-      if (status == kUnset || status == kStopped) {
-        if (status == kUnset)
-          status = kSurrender;
-        fout = best;
-        double gg = 0.0;
-        for (int i = t; i < D; i += kBlock)
-          gg = fma(g[i], g[i], gg);
-        gout = sqrt(grp.sum(gg));
-      }
-      if (out.x)
-        for (int i = t; i < D; i += kBlock)
-          out.x[run * D + i] = x[i];
-      if (t == 0) {
-        if (out.fval)
-          out.fval[run] = fout;
-        if (out.status)
-          out.status[run] = status;
-        if (out.iter)
-          out.iter[run] = iter;
-        if (out.gnorm)
-          out.gnorm[run] = gout;
-        if (out.counters) {
-          out.counters[3 * run + 0] = executed >= 0 ? executed : iter;
-          out.counters[3 * run + 1] = n_eval;
-          out.counters[3 * run + 2] = n_grad;
+          partU[q * D + i] = au;
+          partH[q * D + i] = ah;
         }
       }
       __syncthreads();
+      double yu_part = 0.0;
+      for (int i = t; i < D; i += kBlock) {
+        double au = 0.0, ah = 0.0;
+        for (int q = 0; q < Q; ++q) {
+          au += partU[q * D + i];
+          ah += partH[q * D + i];
+        }
+        u[i] = au;
+        h[i] = ah;
+        yu_part = fma(y[i], au, yu_part);
+      }
+      if (!skipped) {
+        const double yu = grp.sum(yu_part);
+        const double rho = 1.0 / sy;
+        const double hb = 0.5 * rho * fma(rho, yu, 1.0);
+        double wg = 0.0, sg2 = 0.0;
+        for (int i = t; i < D; i += kBlock) {
+          const double wi = fma(hb, s[i], -rho * u[i]);
+          w[i] = wi;
+          wg = fma(wi, gnext[i], wg);
+          sg2 = fma(s[i], gnext[i], sg2);
+        }
+        double v[2] = {wg, sg2};
+        grp.template sum<2>(v); // barriers publish w
+        // sweep 2: H += s w^T + w s^T
+        for (int e = t; e < D * D; e += kBlock) {
+          const int i = e / D, j = e - (e / D) * D;
+          H[e] += __dadd_rn(__dmul_rn(s[i], w[j]), __dmul_rn(w[i], s[j]));
+        }
+        for (int i = t; i < D; i += kBlock)
+          p[i] = -(h[i] + s[i] * v[0] + w[i] * v[1]);
+      } else {
+        for (int i = t; i < D; i += kBlock)
+          p[i] = -h[i];
+      }
+      if (take) {
+        best = fnew;
+        for (int i = t; i < D; i += kBlock) {
+          x[i] = xn[i];
+          g[i] = gn[i];
+        }
+      }
+      // one reduction: ||g||, the next g.p and the stop flag for the next
+      // iteration's check
+      double v3[3] = {0.0, 0.0, t == 0 ? (double)load_stop(ctl) : 0.0};
+      for (int i = t; i < D; i += kBlock) {
+        v3[0] = fma(g[i], g[i], v3[0]);
+        v3[1] = fma(g[i], p[i], v3[1]);
+      }
+      grp.template sum<3>(v3);
+      const double gnrm = sqrt(v3[0]);
+      ddir = v3[1];
+      stop = v3[2] != 0.0;
+      if (!isfinite(gnrm) || !isfinite(fnew)) {
+        status = kNonFinite;
+        fout = fnew;
+        gout = gnrm;
+        break;
+      }
+      if (gnrm < prm.tol) {
+        if (t == 0)
+          note_converged(ctl, prm.required);
+        status = kConverged;
+        fout = best;
+        gout = gnrm;
+        break;
+      }
+      if (!take && skipped && !(prm.flags & kFlagNoFixedPoint)) {
+        executed = iter + 1;
+        iter = prm.max_iter;
+        break;
+      }
     }
+    if (status == kUnset || status == kStopped) {
+      if (status == kUnset)
+        status = kSurrender;
+      fout = best;
+      double gg = 0.0;
+      for (int i = t; i < D; i += kBlock)
+        gg = fma(g[i], g[i], gg);
+      gout = sqrt(grp.sum(gg));
+    }
+    if (out.x)
+      for (int i = t; i < D; i += kBlock)
+        out.x[run * D + i] = x[i];
+    if (t == 0) {
+      if (out.fval)
+        out.fval[run] = fout;
+      if (out.status)
+        out.status[run] = status;
+      if (out.iter)
+        out.iter[run] = iter;
+      if (out.gnorm)
+        out.gnorm[run] = gout;
+      if (out.counters) {
+        out.counters[3 * run + 0] = executed >= 0 ? executed : iter;
+        out.counters[3 * run + 1] = n_eval;
+        out.counters[3 * run + 2] = n_grad;
+      }
+    }
+    __syncthreads();
   }
 
   template <class F, int D, bool Adjoint, int kBlock>

@@ -54,7 +54,7 @@ namespace zb {
     const int b = dim <= 64 ? 256 : 512;
     const int q = b >= dim ? b / dim : 1;
     const size_t d =
-      (size_t)dim * dim + 11 * dim + 2 * q * dim + 32 * 8 + b + 4;
+      (size_t)dim * dim + 11 * dim + 2 * q * dim + 32 * 8 + b + 8 + 4;
     return d * sizeof(double) <= kSmemLimit;
   }
 

@@ -133,4 +133,83 @@ namespace zb {
     }
   };
 
+  // The block split into equal groups of `gsize` threads (a multiple of 32),
+  // group g = threadIdx.x / gsize; threads past the last whole group form an
+  // idle group whose members have rank >= gsize.  Every thread of the block
+  // must call sum() together (it contains block barriers); each group gets
+  // its own total, identical in all its members.  `red` holds 32 * 8
+  // doubles.
+  struct CtaSubGroup {
+    double* red;
+    double* scratch;
+    int gsize;
+
+    __device__ __forceinline__ int
+    group() const
+    {
+      return (int)threadIdx.x / gsize;
+    }
+    __device__ __forceinline__ int
+    rank() const
+    {
+      return (int)threadIdx.x % gsize;
+    }
+    __device__ __forceinline__ int
+    size() const
+    {
+      return gsize;
+    }
+    __device__ __forceinline__ void
+    sync() const
+    {
+      __syncthreads();
+    }
+    template <int K>
+    __device__ __forceinline__ void
+    sum(double (&v)[K]) const
+    {
+      static_assert(K <= 8, "at most 8 simultaneous sums");
+#pragma unroll
+      for (int m = 16; m > 0; m >>= 1)
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          v[k] += __shfl_xor_sync(0xffffffffu, v[k], m);
+      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          red[warp * 8 + k] = v[k];
+      __syncthreads();
+      const int wpg = gsize >> 5, w0 = group() * wpg;
+      const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        double a = 0.0;
+        for (int w = 0; w < wpg; ++w)
+          if (w0 + w < nw)
+            a += red[(w0 + w) * 8 + k];
+        v[k] = a;
+      }
+      __syncthreads();
+    }
+    __device__ __forceinline__ double
+    sum(double v) const
+    {
+      double a[1] = {v};
+      sum<1>(a);
+      return a[0];
+    }
+    // value of member `src` of this thread's group, to the whole group
+    __device__ __forceinline__ double
+    bcast(double v, int src) const
+    {
+      if (rank() == src)
+        scratch[group()] = v;
+      __syncthreads();
+      const double r = scratch[group()];
+      __syncthreads();
+      return r;
+    }
+  };
+
 } // namespace zb
