@@ -170,6 +170,26 @@ int zeus_pso_device(const zeus_problem* problem, uint64_t seed, int64_t n,
                     double* d_pbest_f, double* d_gbest, void* d_workspace,
                     size_t workspace_bytes, void* stream);
 
+/* No counterpart in the reference (its pso::launch allocates its buffers
+ * itself, pso.cuh:211-241).  zeus_pso_device without the workspace, for
+ * callers that cannot allocate device memory where they seed a swarm (an
+ * allocator owned by another framework, allocation-free real-time loops,
+ * hosts that must not let an allocation synchronize the device).  The swarm
+ * state lives in one 8 MiB array compiled into the library, which every GPU
+ * that loads the library keeps until the process exits; calls needing more
+ * (zeus_pso_workspace_size(n, dim) > 8 MiB) are rejected with
+ * ZEUS_E_WORKSPACE.  The first call on a device looks the array's device
+ * address up (cudaGetSymbolAddress), so make that first call before any
+ * stream capture.  All calls share the array and it keeps the last call's
+ * contents; each call clears what must start at zero, but calls that
+ * overlap on the GPU race on it: serialize them.  Outputs as for
+ * zeus_pso_device. */
+int zeus_pso_device_noalloc(const zeus_problem* problem, uint64_t seed,
+                            int64_t n, double lower, double upper,
+                            int32_t iters, double w, double c1, double c2,
+                            double* d_pbest_x, double* d_pbest_f,
+                            double* d_gbest, void* stream);
+
 /* ---- BFGS -----------------------------------------------------------
  * Replaces bfgs::sequential::launch / bfgs::parallel::launch
  * (bfgs_sequential.cuh:384-589, bfgs_parallel.cuh:301-472) and their

@@ -139,6 +139,11 @@ SIGNATURES = {
          C.c_int32, C.c_double, C.c_double, C.c_double, _P, _P, _P, _P,
          C.c_size_t, _P],
     ),
+    "zeus_pso_device_noalloc": (
+        C.c_int,
+        [C.POINTER(Problem), C.c_uint64, C.c_int64, C.c_double, C.c_double,
+         C.c_int32, C.c_double, C.c_double, C.c_double, _P, _P, _P, _P],
+    ),
     "zeus_bfgs_workspace_size": (
         C.c_size_t, [C.POINTER(Problem), C.POINTER(BfgsConfig), C.c_int64]),
     "zeus_bfgs_device": (

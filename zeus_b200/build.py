@@ -42,6 +42,7 @@ UNITS = [
     ("zb_fast_tile.cu", []),
     ("zb_fast_cta.cu", []),
     ("zb_batch.cu", []),
+    ("zb_noalloc.cu", ["-fmad=false"]),
     ("zb_runtime.cu", []),
 ]
 
