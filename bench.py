@@ -310,6 +310,26 @@ def run_gpu(args, rank, world, local_rank):
             cfg_fast = zb.make_config(j.max_iter, j.required, j.tol, "fast", "adjoint")
             s["run"] = BfgsRun(dp, j.n, cfg_fast, device=dev)
         state.append(s)
+    # layout autotuner: every class that is not CTA-sized gets its fastest
+    # built layout recorded before anything is timed (the batch and the
+    # standalone launches read the table)
+    tuned = {}
+    if not args.no_autotune:
+        for s in state:
+            j, obj = s["job"], s["obj"]
+            if obj.dim > 32:
+                continue
+            ns = min(j.n, 16384)
+            if j.runs_per_instance:
+                ns = max(j.runs_per_instance, ns // j.runs_per_instance * j.runs_per_instance)
+                # one data instance is enough to tune on
+                prob_obj = zb.PoissonNLL(obj.idata[:s["nbins"]], obj.data[:s["nbins"]])
+            else:
+                prob_obj = obj
+            lay, tile, ms = zb.autotune(prob_obj, n_sample=ns, max_iter=min(j.max_iter, 300),
+                                        tol=j.tol, lower=j.lo, upper=j.hi, device=dev)
+            tuned[j.name] = {"layout": ["auto", "thread", "tile", "cta"][lay], "tile": tile,
+                             "sample_ms": ms}
     batch = Batch([s["bj"] for s in state], jobs[0].max_iter, jobs[0].tol) if wl["batch"] else None
 
     def gen_starts(s):
@@ -527,7 +547,7 @@ def run_gpu(args, rank, world, local_rank):
             "data": "synthetic",
             "config": {"workload": args.workload, "description": wl["desc"],
                        "gradient": "adjoint", "mode": "fast",
-                       "batched": bool(wl["batch"]),
+                       "batched": bool(wl["batch"]), "autotuned_layouts": tuned,
                        "converged_per_step": conv_all,
                        "runs_per_step": sum(j.n for j in jobs) * world,
                        "l2": "1 GiB buffer written between timed steps",
@@ -716,6 +736,7 @@ def main():
     ap.add_argument("--gradient", default="adjoint", choices=["adjoint", "dual"])
     ap.add_argument("--seed", type=int, default=42)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-plain", action="store_true",
                     help="skip the plain dual-AD comparison")
     ap.add_argument("--plain-steps", type=int, default=1)

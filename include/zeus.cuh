@@ -326,7 +326,8 @@ namespace zeus {
       } else {
         static_assert(D <= 160, "dimensions above 160 are not supported");
         constexpr int B = D <= 64 ? 256 : 512;
-        const size_t smem = sizeof(double) * zb::cta_smem_doubles<(int)D>(B);
+        const size_t smem =
+          sizeof(double) * zb::cta_smem_doubles<F, (int)D, kAdj>(B);
         auto k = zb::bfgs_cta_kernel<F, (int)D, kAdj, B>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);

@@ -131,7 +131,7 @@ namespace zb {
           using F = decltype(f);
           constexpr int D = (int)F::arity;
           if constexpr (D >= kBatchCtaMinDim &&
-                        sizeof(double) * cta_smem_doubles<D>(kBatchBlock) <=
+                        sizeof(double) * cta_smem_doubles<F, D, true>(kBatchBlock) <=
                           227 * 1024)
             cta_run<F, D, true, kBatchBlock>(instance_for(f, c, r), sm, prm,
                                              c.starts + r * D, r, c.out, c.ctl);
@@ -173,7 +173,7 @@ namespace zb {
             }
           }
         } else if constexpr (D < kBatchCtaMinDim) {
-          constexpr unsigned W = batch_widths(D);
+          constexpr unsigned W = batch_widths(F::kind, D);
           switch (c.tile) {
 #define ZB_TS(K)                                                               \
   case (1 << K):                                                               \
@@ -194,11 +194,12 @@ namespace zb {
   }
 
   namespace {
+    // shared memory of a CTA-layout class (the Gaussian's trials carry the
+    // gradient and need no per-warp trial points)
     size_t
-    cta_doubles_rt(int d, int block)
+    cta_doubles_rt(int kind, int d, int block)
     {
-      const int q = block >= d ? block / d : 1;
-      return (size_t)d * d + 11 * d + 2 * q * d + 32 * 8 + block + 8 + 4;
+      return cta_smem_doubles_rt(d, block, kind != ZEUS_OBJ_GAUSSIAN);
     }
 
     bool
@@ -210,10 +211,10 @@ namespace zb {
         return dim <= kBatchThreadMaxDim;
       if (layout == ZEUS_LAYOUT_TILE)
         return tile >= 2 && tile <= 32 && !(tile & (tile - 1)) &&
-               ((batch_widths(dim) >> __builtin_ctz((unsigned)tile)) & 1u);
+               ((batch_widths(kind, dim) >> __builtin_ctz((unsigned)tile)) & 1u);
       if (layout == ZEUS_LAYOUT_CTA)
         return dim >= kBatchCtaMinDim &&
-               cta_doubles_rt(dim, kBatchBlock) * sizeof(double) <= 227 * 1024;
+               cta_doubles_rt(kind, dim, kBatchBlock) * sizeof(double) <= 227 * 1024;
       return false;
     }
 
@@ -233,7 +234,7 @@ namespace zb {
         return;
       }
       if (dim < kBatchCtaMinDim) {
-        const unsigned w = batch_widths(dim);
+        const unsigned w = batch_widths(kind, dim);
         for (int k = 1; k <= 5; ++k)
           if ((w >> k) & 1u) {
             *layout = ZEUS_LAYOUT_TILE;
@@ -365,7 +366,7 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
       b.nll_bins = bins;
     }
     if (layout == ZEUS_LAYOUT_CTA)
-      smem_cta = std::max(smem_cta, cta_doubles_rt(p.dim, kBatchBlock));
+      smem_cta = std::max(smem_cta, cta_doubles_rt(p.kind, p.dim, kBatchBlock));
     if (layout == ZEUS_LAYOUT_TILE)
       smem_tile = std::max(smem_tile, batch_tile_buf_doubles(p.dim, tile));
     hc.push_back(b);

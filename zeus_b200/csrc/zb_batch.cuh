@@ -53,19 +53,22 @@ namespace zb {
     BatchClass c[kMaxBatchClasses];
   };
 
-  // Tile widths compiled into the batch kernel for a dimension: rows of H
-  // of at most 32 doubles per lane (the kernel is limited to 128 registers
-  // per thread by its 512-thread, one-block-per-SM launch bounds).
+  // Tile widths compiled into the batch kernel for an objective and
+  // dimension: rows of H of at most 32 doubles per lane (the kernel is
+  // limited to 128 registers per thread by its 512-thread,
+  // one-block-per-SM launch bounds); wider than 2*D only for the objectives
+  // whose cooperative evaluation splits bins or matrix rows.
   __host__ __device__ constexpr unsigned
-  batch_widths(int d)
+  batch_widths(int kind, int d)
   {
     unsigned m = 0;
     if (d > 32)
       return 0;
+    const bool wide = kind == ZEUS_OBJ_POISSON_NLL || kind == ZEUS_OBJ_GAUSSIAN;
     for (int k = 1; k <= 5; ++k) {
       const int ts = 1 << k;
       const int r = (d + ts - 1) / ts;
-      if (r * d <= 32 && ts <= 2 * d)
+      if (r * d <= 32 && (wide || ts <= 2 * d))
         m |= 1u << k;
     }
     return m;

@@ -328,29 +328,31 @@ namespace zb {
 
   // ---------------------------------------------------------------- CTA
   // Shared-memory layout (doubles): H[D*D] | 11 vectors of D | partial sums
-  // 2*Q*D (also the line-search trial points) | reduction 32*8 | scratch
-  // blockDim | trial values 8 | flags 4.
-  template <int D>
+  // 2*Q*D | reduction buffers kCtaRedDoubles | scratch blockDim | trial
+  // values 2*32 | flags 4 | (warp trials) one trial point per warp,
+  // (blockDim/32)*D.
+  __host__ __device__ constexpr size_t
+  cta_smem_doubles_rt(int d, int block, bool warp_trials)
+  {
+    const int q = block >= d ? block / d : 1;
+    return (size_t)d * d + 11 * d + 2 * q * d + kCtaRedDoubles + block + 64 + 4 +
+           (warp_trials ? (size_t)(block / 32) * d : 0);
+  }
+
+  // Line-search trials are evaluated one per warp, all warps at once, unless
+  // a trial carries a gradient (the Gaussian's C x needs the whole block).
+  template <class F, bool Adjoint>
+  __host__ __device__ constexpr bool
+  cta_warp_trials()
+  {
+    return !(Adjoint && TrialsWithGradient<F>);
+  }
+
+  template <class F, int D, bool Adjoint>
   __host__ __device__ constexpr size_t
   cta_smem_doubles(int block)
   {
-    const int q = block >= D ? block / D : 1;
-    return (size_t)D * D + 11 * D + 2 * q * D + 32 * 8 + block + 8 + 4;
-  }
-
-  // Line-search trials evaluated at once in the CTA layout: the block splits
-  // into groups of round32(D) threads, one trial point each; none when the
-  // trials carry a gradient (the Gaussian's C x needs the whole block).
-  template <class F, int D, bool Adjoint, int kBlock>
-  __host__ __device__ constexpr int
-  cta_trials_per_round()
-  {
-    constexpr int dr = (D + 31) / 32 * 32;
-    constexpr int k = kBlock / dr;
-    if constexpr (Adjoint && TrialsWithGradient<F>)
-      return 1;
-    else
-      return k < 1 ? 1 : (k > 8 ? 8 : k);
+    return cta_smem_doubles_rt(D, block, cta_warp_trials<F, Adjoint>());
   }
 
   // One run on the whole block (blockDim.x == kBlock): `sm` holds
@@ -363,9 +365,8 @@ namespace zb {
   {
     constexpr int Q = kBlock >= D ? kBlock / D : 1;
     constexpr bool kTrialGrad = Adjoint && TrialsWithGradient<F>;
-    constexpr int DR = (D + 31) / 32 * 32;
-    constexpr int KT = cta_trials_per_round<F, D, Adjoint, kBlock>();
-    static_assert(KT <= Q, "trial points reuse the partial-sum area");
+    constexpr bool kWarpTrials = cta_warp_trials<F, Adjoint>();
+    constexpr int NW = kBlock / 32;
     double* H = sm;
     double* x = H + D * D;
     double* g = x + D;
@@ -381,8 +382,9 @@ namespace zb {
     double* partU = gt + D;
     double* partH = partU + Q * D;
     double* red = partH + Q * D;
-    double* scratch = red + 32 * 8;
-    double* trial_f = scratch + kBlock;
+    double* scratch = red + kCtaRedDoubles;
+    double* trial_f = scratch + kBlock; // 2 x 32: alternate rounds
+    double* trial_x = trial_f + 64 + 4; // NW x D when kWarpTrials
     CtaGroup grp{red, scratch};
     const int t = threadIdx.x;
 
@@ -424,27 +426,37 @@ namespace zb {
       // else alpha = 2^-20 (utils.cuh:376-412)
       double fnew = 0.0;
       bool have_grad = false;
-      if constexpr (KT > 1) {
-        const int q = t / DR, j = t % DR;
-        const bool inq = q < KT;
-        double* tx = partU + (inq ? q : 0) * D;
-        int found = -1;
+      if constexpr (kWarpTrials) {
+        // warp w evaluates trial k = r0 + w of each round on its own copy of
+        // the trial point (shuffle reductions, no block barrier); one
+        // barrier per round publishes the values, which every thread scans
+        // in trial order
+        const int warp = t >> 5, lane = t & 31;
+        double* wx = trial_x + warp * D;
+        const TileGroup<32> wg(cg::tiled_partition<32>(cg::this_thread_block()),
+                               scratch + warp * 32);
+        int found = -1, round = 0;
         double alpha = 0.0;
-        for (int r0 = 0; found < 0; r0 += KT) {
-          const int k = r0 + q;
-          if (inq && j < D && k <= kLineSearchTrials)
-            tx[j] = fma(ldexp(1.0, -k), p[j], x[j]);
+        for (int r0 = 0; found < 0; r0 += NW, ++round) {
+          const int k = r0 + warp;
+          double f1 = 0.0;
+          if (k <= kLineSearchTrials) {
+            const double ak = ldexp(1.0, -k);
+            for (int i = lane; i < D; i += 32)
+              wx[i] = fma(ak, p[i], x[i]);
+            __syncwarp();
+            f1 = coop_value<F, D>(f, wg, wx);
+            __syncwarp();
+          }
+          double* tf = trial_f + (round & 1) * 32;
+          if (lane == 0)
+            tf[warp] = f1;
           __syncthreads();
-          const CtaSubGroup sg{red, scratch, DR};
-          const double f1 = coop_value<F, D>(f, sg, tx);
-          if (inq && j == 0)
-            trial_f[q] = f1;
-          __syncthreads();
-          for (int qq = 0; qq < KT; ++qq) {
-            const int kk = r0 + qq;
+          for (int w = 0; w < NW; ++w) {
+            const int kk = r0 + w;
             if (kk > kLineSearchTrials)
               break;
-            const double fk = trial_f[qq], ak = ldexp(1.0, -kk);
+            const double fk = tf[w], ak = ldexp(1.0, -kk);
             if (kk == kLineSearchTrials ||
                 (fk <= best + kArmijoC1 * ak * ddir && fk < best)) {
               found = kk;

@@ -21,7 +21,7 @@ namespace zb {
                const RunOut& out, Control* ctl, cudaStream_t st)
     {
       constexpr int B = cta_block<D>();
-      const size_t smem = sizeof(double) * cta_smem_doubles<D>(B);
+      const size_t smem = sizeof(double) * cta_smem_doubles<F, D, Adj>(B);
       auto kern = bfgs_cta_kernel<F, D, Adj, B>;
       int rc = cuda_fail(cudaFuncSetAttribute(
                            kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -52,10 +52,8 @@ namespace zb {
     if (!builtin_supported(kind, dim) || dim < kMinCtaDim)
       return false;
     const int b = dim <= 64 ? 256 : 512;
-    const int q = b >= dim ? b / dim : 1;
-    const size_t d =
-      (size_t)dim * dim + 11 * dim + 2 * q * dim + 32 * 8 + b + 8 + 4;
-    return d * sizeof(double) <= kSmemLimit;
+    // the larger of the two variants (warp trials need an extra D per warp)
+    return cta_smem_doubles_rt(dim, b, true) * sizeof(double) <= kSmemLimit;
   }
 
   int
@@ -68,7 +66,7 @@ namespace zb {
       using F = decltype(f);
       constexpr int D = (int)F::arity;
       if constexpr (D >= kMinCtaDim &&
-                    sizeof(double) * cta_smem_doubles<D>(cta_block<D>()) <=
+                    sizeof(double) * cta_smem_doubles_rt(D, cta_block<D>(), true) <=
                       kSmemLimit) {
         if (adjoint)
           return launch_one<F, D, true>(f, prm, starts, out, ctl, st);

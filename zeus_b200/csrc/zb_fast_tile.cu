@@ -5,17 +5,21 @@
 namespace zb {
 
   namespace {
-    // widths built for a dimension: H rows per lane R*D <= 64 doubles
+    // widths built for an objective and dimension: H rows per lane R*D <=
+    // 64 doubles; wider than 2*D only where the cooperative evaluation
+    // splits something other than the coordinates (the NLL's bins, the
+    // Gaussian's C x)
     constexpr unsigned
-    widths_for(int d)
+    widths_for(int kind, int d)
     {
       unsigned m = 0;
       if (d > 32)
         return 0;
+      const bool wide = kind == ZEUS_OBJ_POISSON_NLL || kind == ZEUS_OBJ_GAUSSIAN;
       for (int k = 1; k <= 5; ++k) {
         const int ts = 1 << k;
         const int r = (d + ts - 1) / ts;
-        if (r * d <= 64 && ts <= 2 * d)
+        if (r * d <= 64 && (wide || ts <= 2 * d))
           m |= 1u << k;
       }
       return m;
@@ -43,7 +47,7 @@ namespace zb {
   unsigned
   tile_widths(int kind, int dim)
   {
-    return builtin_supported(kind, dim) ? widths_for(dim) : 0u;
+    return builtin_supported(kind, dim) ? widths_for(kind, dim) : 0u;
   }
 
   int
@@ -55,7 +59,7 @@ namespace zb {
     return visit_objective(o, [&](auto f) -> int {
       using F = decltype(f);
       constexpr int D = (int)F::arity;
-      constexpr unsigned W = widths_for(D);
+      constexpr unsigned W = widths_for(F::kind, D);
       switch (tile) {
 #define ZB_TS(K)                                                               \
   case (1 << K):                                                               \

@@ -65,12 +65,18 @@ namespace zb {
     }
   };
 
-  // `red` points at 32 * 8 doubles of shared memory reserved for the
-  // group's reductions (32 warps x up to 8 simultaneous sums); the block
-  // size must be a multiple of 32.
+  // `red` points at kCtaRedDoubles doubles of shared memory reserved for the
+  // group's reductions: two buffers of 32 warps x 8 values used in turn --
+  // every thread runs the same sequence of sums, so a buffer is rewritten
+  // only two sums later, after the barrier of the sum in between, when every
+  // thread has finished reading it: one barrier per sum -- plus one slot for
+  // bcast().  The block size must be a multiple of 32.
+  inline constexpr int kCtaRedDoubles = 2 * 32 * 8 + 8;
+
   struct CtaGroup {
     double* red;
     double* scratch;
+    mutable int parity = 0;
 
     __device__ __forceinline__ int
     rank() const
@@ -99,7 +105,8 @@ namespace zb {
           v[k] += __shfl_xor_sync(0xffffffffu, v[k], m);
       const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
       const int nw = (blockDim.x + 31) >> 5;
-      double* buf = red;
+      double* buf = red + parity * (32 * 8);
+      parity ^= 1;
       if (lane == 0)
 #pragma unroll
         for (int k = 0; k < K; ++k)
@@ -112,7 +119,6 @@ namespace zb {
           a += buf[w * 8 + k];
         v[k] = a;
       }
-      __syncthreads(); // everyone has read buf before it is reused
     }
     __device__ __forceinline__ double
     sum(double v) const
@@ -124,89 +130,11 @@ namespace zb {
     __device__ __forceinline__ double
     bcast(double v, int src) const
     {
+      double* slot = red + 2 * 32 * 8;
       if ((int)threadIdx.x == src)
-        red[0] = v;
+        slot[0] = v;
       __syncthreads();
-      const double r = red[0];
-      __syncthreads();
-      return r;
-    }
-  };
-
-  // The block split into equal groups of `gsize` threads (a multiple of 32),
-  // group g = threadIdx.x / gsize; threads past the last whole group form an
-  // idle group whose members have rank >= gsize.  Every thread of the block
-  // must call sum() together (it contains block barriers); each group gets
-  // its own total, identical in all its members.  `red` holds 32 * 8
-  // doubles.
-  struct CtaSubGroup {
-    double* red;
-    double* scratch;
-    int gsize;
-
-    __device__ __forceinline__ int
-    group() const
-    {
-      return (int)threadIdx.x / gsize;
-    }
-    __device__ __forceinline__ int
-    rank() const
-    {
-      return (int)threadIdx.x % gsize;
-    }
-    __device__ __forceinline__ int
-    size() const
-    {
-      return gsize;
-    }
-    __device__ __forceinline__ void
-    sync() const
-    {
-      __syncthreads();
-    }
-    template <int K>
-    __device__ __forceinline__ void
-    sum(double (&v)[K]) const
-    {
-      static_assert(K <= 8, "at most 8 simultaneous sums");
-#pragma unroll
-      for (int m = 16; m > 0; m >>= 1)
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-          v[k] += __shfl_xor_sync(0xffffffffu, v[k], m);
-      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-      if (lane == 0)
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-          red[warp * 8 + k] = v[k];
-      __syncthreads();
-      const int wpg = gsize >> 5, w0 = group() * wpg;
-      const int nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        double a = 0.0;
-        for (int w = 0; w < wpg; ++w)
-          if (w0 + w < nw)
-            a += red[(w0 + w) * 8 + k];
-        v[k] = a;
-      }
-      __syncthreads();
-    }
-    __device__ __forceinline__ double
-    sum(double v) const
-    {
-      double a[1] = {v};
-      sum<1>(a);
-      return a[0];
-    }
-    // value of member `src` of this thread's group, to the whole group
-    __device__ __forceinline__ double
-    bcast(double v, int src) const
-    {
-      if (rank() == src)
-        scratch[group()] = v;
-      __syncthreads();
-      const double r = scratch[group()];
+      const double r = slot[0];
       __syncthreads();
       return r;
     }
