@@ -168,7 +168,8 @@ def workloads():
         "dijet": dict(
             desc="512 Poisson toy dijet spectra x 256 uniform starts in [0,10]^4, "
                  "4-parameter NLL, one persistent batch of 131072 runs, <=10000 iters, "
-                 "tol 1e-8, stop-early off",
+                 "tol 1e-8, stop-early off; then d(fit)/d(counts) of each toy's best "
+                 "fit (implicit-function adjoint, one extra launch)",
             batch=True,
             jobs=[Job("dijet", lambda: dijet_objective(), 131072, 0.0, 10.0, -1, 10000,
                       1 << 30, runs_per_instance=256)]),
@@ -306,6 +307,11 @@ def run_gpu(args, rank, world, local_rank):
                             ws=torch.empty((max(pws, 1),), dtype=torch.uint8, device=dev),
                             wsz=pws)
         s["bj"] = BatchJob(dp, starts, required=j.required, runs_per_instance=j.runs_per_instance)
+        if j.runs_per_instance and obj.kind == 4:
+            # d(fitted parameters)/d(bin counts) of every toy's best fit
+            toys = j.n // j.runs_per_instance
+            s["sens"] = (torch.empty((toys, 6), dtype=torch.float64, device=dev),
+                         torch.empty((toys, 4, s["nbins"]), dtype=torch.float64, device=dev))
         if not j.runs_per_instance:
             cfg_fast = zb.make_config(j.max_iter, j.required, j.tol, "fast", "adjoint")
             s["run"] = BfgsRun(dp, j.n, cfg_fast, device=dev)
@@ -369,6 +375,13 @@ def run_gpu(args, rank, world, local_rank):
         e1.record(stream)
         for s, o in zip(state, outs):
             launches += census(s, o)
+            if "sens" in s:
+                best, sens = s["sens"]
+                prob = s["bj"].c().problem
+                zb.check(L.zeus_nll_sensitivity_device(
+                    C.byref(prob), best.shape[0], s["job"].runs_per_instance,
+                    o.fval.data_ptr(), o.x.data_ptr(), best.data_ptr(), sens.data_ptr(), sh))
+                launches += 1
         return (e0, e1), launches, outs
 
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.float32, device=dev)

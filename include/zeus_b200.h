@@ -237,6 +237,23 @@ int zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
                       const zeus_bfgs_config* config, void* d_workspace,
                       size_t workspace_bytes, void* stream);
 
+/* ---- fit sensitivities ----------------------------------------------------
+ * No counterpart in the reference (its dijet fit stops at the minimum,
+ * examples/fit_dijet_spectrum.cu:162-221).  For a Poisson NLL batch with
+ * n_instances toy spectra (problem->data / idata: ndata centres and counts
+ * per toy, one toy after another) and runs_per_instance runs per toy
+ * (d_fval and d_x hold n_instances * runs_per_instance runs):
+ * picks each toy's best run (lowest fval, lowest index on ties) and writes
+ * d_best[toy*6 + {0..5}] = {fval, a, b, c, d, run index} and the implicit-
+ * function derivatives of the fitted parameters with respect to the bin
+ * counts, d_sens[(toy*4 + param)*ndata + bin] = d p_param / d k_bin
+ * = (H^-1 J_bin)_param, H the exact Hessian of the NLL at the fit, J_bin =
+ * d ln lambda_bin / dp. */
+int zeus_nll_sensitivity_device(const zeus_problem* problem,
+                                int64_t n_instances, int64_t runs_per_instance,
+                                const double* d_fval, const double* d_x,
+                                double* d_best, double* d_sens, void* stream);
+
 /* ---- layout autotuner -------------------------------------------------
  * No reference counterpart (the reference fixes thread-per-run or a tile
  * of min(32, 2^floor(log2 D)) lanes, bfgs_parallel.cuh:57-65).  Times every

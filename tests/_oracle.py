@@ -184,3 +184,66 @@ def dijet_toy(seed=7, nbins=100, total=1e6, p=(1e6, 10.0, 5.0, 0.1)):
     rng = np.random.default_rng(seed)
     k = rng.poisson(lam).astype(np.int32)
     return x, k, lam
+
+
+# ------------------------------------------------------------------ dijet fits
+# The implicit-function adjoint of the binned Poisson fit has no counterpart
+# in the reference (its dijet example stops at the minimum,
+# examples/fit_dijet_spectrum.cu:162-221); these numpy functions are the
+# checker for it: NLL = sum_i lambda_i - k_i ln lambda_i (+ const) with
+# ln lambda = ln a + b ln(1-x) - (c + d ln x) ln x.
+def nll_parts(x, k, p):
+    """(lambda, J = d ln lambda / dp (4, nbins), gradient, exact Hessian)."""
+    a, b, c, d = p
+    lx, l1 = np.log(x), np.log1p(-x)
+    lam = np.exp(np.log(a) + b * l1 - (c + d * lx) * lx)
+    J = np.stack([np.full_like(x, 1.0 / a), l1, -lx, -lx * lx])
+    r = lam - k
+    grad = J @ r
+    H = (J * lam) @ J.T
+    H[0, 0] -= r.sum() / (a * a)
+    return lam, J, grad, H
+
+
+def nll_value(x, k, p):
+    a, b, c, d = p
+    lx, l1 = np.log(x), np.log1p(-x)
+    ll = np.log(a) + b * l1 - (c + d * lx) * lx
+    return float(np.sum(np.exp(ll) - k * ll))
+
+
+def nll_newton_fit(x, k, p0, iters=100):
+    """The fit by Newton's method in theta = (ln a, b, c, d), where ln lambda
+    is linear in theta (a Poisson log-linear model: the NLL is convex and its
+    Hessian sum lambda J J^T positive definite), with step halving; returns
+    p = (a, b, c, d)."""
+    lx, l1 = np.log(x), np.log1p(-x)
+    Jt = np.stack([np.ones_like(x), l1, -lx, -lx * lx])
+    k = np.asarray(k, dtype=np.float64)
+
+    def f(t):
+        ll = t @ Jt
+        return float(np.sum(np.exp(ll) - k * ll))
+
+    t = np.array([np.log(p0[0]), p0[1], p0[2], p0[3]], dtype=np.float64)
+    fv = f(t)
+    for _ in range(iters):
+        lam = np.exp(t @ Jt)
+        step = np.linalg.solve((Jt * lam) @ Jt.T, Jt @ (lam - k))
+        h = 1.0
+        while h > 1e-8 and f(t - h * step) > fv:
+            h *= 0.5
+        t_new = t - h * step
+        f_new = f(t_new)
+        done = f_new >= fv and h < 1.0
+        if f_new <= fv:
+            t, fv = t_new, f_new
+        if done or np.all(np.abs(h * step) <= 1e-15 * np.maximum(np.abs(t), 1.0)):
+            break
+    return np.array([np.exp(t[0]), t[1], t[2], t[3]])
+
+
+def nll_sensitivity(x, k, p):
+    """d p_hat / d k_j = H^-1 J_j for every bin j, shape (4, nbins)."""
+    _, J, _, H = nll_parts(x, k, p)
+    return np.linalg.solve(H, J)

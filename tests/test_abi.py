@@ -64,6 +64,26 @@ def test_invalid_arguments_fail_loudly_without_gpu():
                               C.byref(zb.RunOutputs()), None, None, 0, None) == zb.E_INVALID
 
 
+def test_nll_sensitivity_rejects_bad_input_without_gpu():
+    L = zb.lib()
+    ros = zb.Problem(zb.OBJ_ROSENBROCK, 2, None, None, 0, 0)
+    assert L.zeus_nll_sensitivity_device(C.byref(ros), 1, 4, None, None, None, None,
+                                         None) == zb.E_INVALID
+    assert "Poisson NLL" in zb.last_error()
+    data = (C.c_double * 4)()
+    idata = (C.c_int32 * 4)()
+    nll = zb.Problem(zb.OBJ_POISSON_NLL, 4, C.cast(data, C.c_void_p),
+                     C.cast(idata, C.c_void_p), 4, 0)
+    # runs_per_instance must be positive; buffers are required for n > 0
+    assert L.zeus_nll_sensitivity_device(C.byref(nll), 1, 0, None, None, None, None,
+                                         None) == zb.E_INVALID
+    assert L.zeus_nll_sensitivity_device(C.byref(nll), 1, 4, None, None, None, None,
+                                         None) == zb.E_INVALID
+    # no toys: nothing to do, no device call
+    assert L.zeus_nll_sensitivity_device(C.byref(nll), 0, 4, None, None, None, None,
+                                         None) == zb.OK
+
+
 def test_workspace_sizes():
     L = zb.lib()
     prob = zb.Problem(zb.OBJ_ROSENBROCK, 2, None, None, 0, 0)

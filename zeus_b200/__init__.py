@@ -163,6 +163,8 @@ SIGNATURES = {
     "zeus_batch_device": (
         C.c_int, [C.POINTER(BatchClass), C.c_int32, C.POINTER(BfgsConfig), _P, C.c_size_t,
                   _P]),
+    "zeus_nll_sensitivity_device": (
+        C.c_int, [C.POINTER(Problem), C.c_int64, C.c_int64, _P, _P, _P, _P, _P]),
     "zeus_autotune": (
         C.c_int,
         [C.POINTER(Problem), C.POINTER(BfgsConfig), C.c_int64, C.c_uint64, C.c_double,

@@ -43,6 +43,7 @@ UNITS = [
     ("zb_fast_cta.cu", []),
     ("zb_batch.cu", []),
     ("zb_noalloc.cu", ["-fmad=false"]),
+    ("zb_fit.cu", []),
     ("zb_runtime.cu", []),
 ]
 

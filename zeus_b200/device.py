@@ -178,7 +178,7 @@ class BatchJob:
         prob = self.dp.c()
         if self.rpi and self.dp.idata is not None:
             # ndata is per instance
-            ninst = (self.n + self.rpi - 1) // self.rpi
+            ninst = max(1, (self.n + self.rpi - 1) // self.rpi)
             prob.ndata = self.dp.idata.numel() // ninst
         return BatchClass(prob, self.n, self.rpi, _ptr(self.starts), out,
                           _ptr(self.control), self.required, self.layout, self.tile, 0)
@@ -223,3 +223,20 @@ def autotune(obj, n_sample: int = 2048, max_iter: int = 10000, tol: float = 1e-8
                               C.byref(lay), C.byref(til), C.byref(ms),
                               _stream_handle(stream)))
     return lay.value, til.value, ms.value
+
+
+def nll_sensitivity(job: "BatchJob", stream=None):
+    """d(fitted parameters)/d(bin counts) for every toy of a Poisson NLL batch
+    class: returns (best (toys, 6): fval, a, b, c, d, run; sens (toys, 4,
+    nbins))."""
+    if not job.rpi or job.n % job.rpi:
+        raise ValueError("the class must have runs_per_instance > 0 dividing its runs")
+    toys = job.n // job.rpi
+    prob = job.c().problem
+    dev = job.fval.device
+    best = torch.empty((toys, 6), dtype=torch.float64, device=dev)
+    sens = torch.empty((toys, 4, prob.ndata), dtype=torch.float64, device=dev)
+    check(lib().zeus_nll_sensitivity_device(C.byref(prob), toys, job.rpi,
+                                            _ptr(job.fval), _ptr(job.x), _ptr(best),
+                                            _ptr(sens), _stream_handle(stream)))
+    return best, sens
