@@ -217,7 +217,10 @@ int zeus_bfgs_device(const zeus_problem* problem,
  * after another (Gaussian: dim*dim doubles each; NLL: ndata centres and
  * ndata counts each), run r using instance r / runs_per_instance.
  * Fast mode with adjoint gradients only (config->mode, ->gradient);
- * config->max_iter, ->tolerance and ->flags apply to every class. */
+ * config->max_iter, ->tolerance and ->flags apply to every class;
+ * config->block picks the kernel's block size, 512 or 384 threads (0: 512
+ * when the tile/thread classes hold more than two waves of warps, else
+ * 384, whose threads get more registers). */
 typedef struct zeus_batch_class {
   zeus_problem problem;       /* data on the device */
   int64_t n;                  /* runs */

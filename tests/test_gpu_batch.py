@@ -36,7 +36,8 @@ def test_batch_equals_standalone_launches(cuda):
         st = starts_uniform(100 + i, n, mk().dim, lo, hi)
         sts.append(st)
         jobs.append(BatchJob(mk(), st, layout=lay, tile=tile))
-    b = batch_device(jobs, max_iter=600)
+    # 512-thread blocks: the standalone CTA kernel's block at dim 128
+    b = batch_device(jobs, max_iter=600, block=512)
     torch.cuda.synchronize()
     for (mk, n, lay, tile, _), j, st in zip(MIX, jobs, sts):
         ref = bfgs_device(mk(), st, max_iter=600, layout=lay, tile=tile)
@@ -87,6 +88,19 @@ def test_batch_per_instance_nll_toys(cuda):
         w = host(one)
         for k in got:
             np.testing.assert_array_equal(got[k][t * per:(t + 1) * per], w[k], err_msg=k)
+
+
+def test_batch_block_sizes_agree_on_tile_classes(cuda):
+    """The 384- and 512-thread kernels run the same per-run tile bodies."""
+    st = starts_uniform(9, 500, 8, -5.0, 5.0)
+    outs = []
+    for block in (384, 512):
+        j = BatchJob(zb.Rosenbrock(8), st, layout=zb.LAYOUT_TILE, tile=8)
+        batch_device([j], max_iter=800, block=block)
+        torch.cuda.synchronize()
+        outs.append(host(j))
+    for k in outs[0]:
+        np.testing.assert_array_equal(outs[0][k], outs[1][k], err_msg=k)
 
 
 def test_batch_stop_early_per_class(cuda):

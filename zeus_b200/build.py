@@ -42,6 +42,8 @@ UNITS = [
     ("zb_fast_tile.cu", []),
     ("zb_fast_cta.cu", []),
     ("zb_batch.cu", []),
+    ("zb_batch_512.cu", []),
+    ("zb_batch_384.cu", []),
     ("zb_noalloc.cu", ["-fmad=false"]),
     ("zb_fit.cu", []),
     ("zb_runtime.cu", []),

@@ -1,4 +1,6 @@
-// Persistent batched BFGS kernel and its C ABI (zeus_batch_*).
+// Host side of the persistent batched BFGS (zeus_batch_*): validates the
+// classes, picks layouts and the block size, and launches one of the kernel
+// instantiations (zb_batch_512.cu, zb_batch_384.cu).
 #include <algorithm>
 #include <vector>
 
@@ -7,191 +9,6 @@
 #include "zb_reduce.cuh"
 
 namespace zb {
-
-  namespace {
-
-    // Device-side (kind, dim) -> functor, for the dimensions the library is
-    // built for (the same sets as visit_objective).
-    template <class Fn>
-    __device__ __forceinline__ void
-    batch_visit(const BatchClass& c, Fn&& fn)
-    {
-      switch (c.kind) {
-        case ZEUS_OBJ_ROSENBROCK:
-          switch (c.dim) {
-#define ZB_CASE(D)                                                             \
-  case D:                                                                      \
-    fn(zeus::Rosenbrock<D>{});                                                 \
-    return;
-            ZB_ROSENBROCK_DIMS(ZB_CASE)
-#undef ZB_CASE
-          }
-          return;
-        case ZEUS_OBJ_RASTRIGIN:
-          switch (c.dim) {
-#define ZB_CASE(D)                                                             \
-  case D:                                                                      \
-    fn(zeus::Rastrigin<D>{});                                                  \
-    return;
-            ZB_RASTRIGIN_DIMS(ZB_CASE)
-#undef ZB_CASE
-          }
-          return;
-        case ZEUS_OBJ_ACKLEY:
-          switch (c.dim) {
-#define ZB_CASE(D)                                                             \
-  case D:                                                                      \
-    fn(zeus::Ackley<D>{});                                                     \
-    return;
-            ZB_ACKLEY_DIMS(ZB_CASE)
-#undef ZB_CASE
-          }
-          return;
-        case ZEUS_OBJ_GAUSSIAN:
-          switch (c.dim) {
-#define ZB_CASE(D)                                                             \
-  case D: {                                                                    \
-    zeus::Gaussian<D> g;                                                       \
-    g.C = c.data;                                                              \
-    g.symmetric = (c.flags & 1) != 0;                                          \
-    fn(g);                                                                     \
-    return;                                                                    \
-  }
-            ZB_GAUSSIAN_DIMS(ZB_CASE)
-#undef ZB_CASE
-          }
-          return;
-        case ZEUS_OBJ_POISSON_NLL:
-          if (c.dim == 4) {
-            zeus::PoissonNLL p;
-            p.centres = c.data;
-            p.counts = c.idata;
-            p.bins = c.nll_bins;
-            p.nbins = c.ndata;
-            fn(p);
-          }
-          return;
-      }
-    }
-
-    template <class F>
-    __device__ __forceinline__ F
-    instance_for(const F& f, const BatchClass& c, int64_t run)
-    {
-      return c.runs_per_instance > 0 ? with_instance(f, c, run / c.runs_per_instance)
-                                     : f;
-    }
-
-    template <class F, int D, int TS>
-    __device__ __forceinline__ void
-    drain_tile_class(const F& f, const BatchClass& c, const BfgsParams& prm,
-                     double* warp_buf)
-    {
-      auto tile = cg::tiled_partition<TS>(cg::this_thread_block());
-      const int tin = (int)(threadIdx.x & 31) / TS;
-      double* buf = warp_buf + tin * (4 * D + TS);
-      for (;;) {
-        unsigned long long r = 0;
-        if (tile.thread_rank() == 0)
-          r = atomicAdd(c.queue, 1ull);
-        r = tile.shfl(r, 0);
-        if ((int64_t)r >= c.n)
-          break;
-        tile_run<F, D, TS, true>(instance_for(f, c, (int64_t)r), tile, buf, prm,
-                                 c.starts + (int64_t)r * D, (int64_t)r, c.out,
-                                 c.ctl);
-      }
-    }
-
-  } // namespace
-
-  __global__ void __launch_bounds__(kBatchBlock, 1)
-    bfgs_batch_kernel(const __grid_constant__ BatchTable bt)
-  {
-    const int ncls = bt.ncls;
-    const BatchClass* classes = bt.c;
-    extern __shared__ double sm[];
-    __shared__ unsigned long long sh_run;
-
-    // phase A: CTA-layout classes, one run per block at a time
-    for (int ci = 0; ci < ncls; ++ci) {
-      const BatchClass c = classes[ci];
-      if (c.layout != ZEUS_LAYOUT_CTA)
-        continue;
-      const BfgsParams prm{c.n, bt.max_iter, c.required, bt.tol, bt.flags};
-      for (;;) {
-        if (threadIdx.x == 0)
-          sh_run = atomicAdd(c.queue, 1ull);
-        __syncthreads();
-        const int64_t r = (int64_t)sh_run;
-        __syncthreads();
-        if (r >= c.n)
-          break;
-        batch_visit(c, [&](auto f) {
-          using F = decltype(f);
-          constexpr int D = (int)F::arity;
-          if constexpr (D >= kBatchCtaMinDim &&
-                        sizeof(double) * cta_smem_doubles<F, D, true>(kBatchBlock) <=
-                          227 * 1024)
-            cta_run<F, D, true, kBatchBlock>(instance_for(f, c, r), sm, prm,
-                                             c.starts + r * D, r, c.out, c.ctl);
-        });
-      }
-    }
-    __syncthreads();
-
-    // phase B: each warp drains the tile / thread classes
-    double* warp_buf = nullptr;
-    {
-      // per-warp buffers follow each other; sized by the host for the
-      // widest class of the batch
-      const int warp = threadIdx.x >> 5;
-      size_t stride = 0;
-      for (int ci = 0; ci < ncls; ++ci)
-        if (classes[ci].layout == ZEUS_LAYOUT_TILE)
-          stride = stride > batch_tile_buf_doubles(classes[ci].dim, classes[ci].tile)
-                     ? stride
-                     : batch_tile_buf_doubles(classes[ci].dim, classes[ci].tile);
-      warp_buf = sm + (size_t)warp * stride;
-    }
-    for (int ci = 0; ci < ncls; ++ci) {
-      const BatchClass c = classes[ci];
-      if (c.layout == ZEUS_LAYOUT_CTA)
-        continue;
-      const BfgsParams prm{c.n, bt.max_iter, c.required, bt.tol, bt.flags};
-      batch_visit(c, [&](auto f) {
-        using F = decltype(f);
-        constexpr int D = (int)F::arity;
-        if (c.layout == ZEUS_LAYOUT_THREAD) {
-          if constexpr (D <= kBatchThreadMaxDim) {
-            for (;;) {
-              const int64_t r = (int64_t)atomicAdd(c.queue, 1ull);
-              if (r >= c.n)
-                break;
-              thread_run<F, D, true>(instance_for(f, c, r), prm,
-                                     c.starts + r * D, r, c.out, c.ctl);
-            }
-          }
-        } else if constexpr (D < kBatchCtaMinDim) {
-          constexpr unsigned W = batch_widths(F::kind, D);
-          switch (c.tile) {
-#define ZB_TS(K)                                                               \
-  case (1 << K):                                                               \
-    if constexpr ((W >> K) & 1u)                                               \
-      drain_tile_class<F, D, (1 << K)>(f, c, prm, warp_buf);                   \
-    break;
-            ZB_TS(1)
-            ZB_TS(2)
-            ZB_TS(3)
-            ZB_TS(4)
-            ZB_TS(5)
-#undef ZB_TS
-          }
-        }
-      });
-      __syncwarp();
-    }
-  }
 
   namespace {
     // shared memory of a CTA-layout class (the Gaussian's trials carry the
@@ -214,7 +31,8 @@ namespace zb {
                ((batch_widths(kind, dim) >> __builtin_ctz((unsigned)tile)) & 1u);
       if (layout == ZEUS_LAYOUT_CTA)
         return dim >= kBatchCtaMinDim &&
-               cta_doubles_rt(kind, dim, kBatchBlock) * sizeof(double) <= 227 * 1024;
+               cta_doubles_rt(kind, dim, kBatchBlockSmall) * sizeof(double) <=
+                 227 * 1024;
       return false;
     }
 
@@ -234,13 +52,20 @@ namespace zb {
         return;
       }
       if (dim < kBatchCtaMinDim) {
+        // one H row per lane (the narrowest such tile), else the widest built
         const unsigned w = batch_widths(kind, dim);
+        int pick = 0;
         for (int k = 1; k <= 5; ++k)
           if ((w >> k) & 1u) {
-            *layout = ZEUS_LAYOUT_TILE;
-            *tile = 1 << k;
-            return;
+            pick = k;
+            if ((1 << k) >= dim)
+              break;
           }
+        if (pick) {
+          *layout = ZEUS_LAYOUT_TILE;
+          *tile = 1 << pick;
+          return;
+        }
       }
       *layout = ZEUS_LAYOUT_CTA;
     }
@@ -318,7 +143,8 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
   auto* queues = reinterpret_cast<unsigned long long*>(ws + off_q);
   std::vector<BatchClass> hc;
   hc.reserve(n_classes);
-  size_t smem_cta = 0, smem_tile = 0;
+  size_t smem_tile = 0;
+  double warp_runs = 0.0;
   for (int i = 0; i < n_classes; ++i) {
     const zeus_batch_class& c = classes[i];
     const zeus_problem& p = c.problem;
@@ -365,12 +191,32 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
         return rc;
       b.nll_bins = bins;
     }
-    if (layout == ZEUS_LAYOUT_CTA)
-      smem_cta = std::max(smem_cta, cta_doubles_rt(p.kind, p.dim, kBatchBlock));
     if (layout == ZEUS_LAYOUT_TILE)
       smem_tile = std::max(smem_tile, batch_tile_buf_doubles(p.dim, tile));
+    // warps' worth of phase-B runs (a tile of TS lanes is TS/32 of a warp)
+    if (layout == ZEUS_LAYOUT_TILE)
+      warp_runs += (double)c.n * tile / 32.0;
+    else if (layout == ZEUS_LAYOUT_THREAD)
+      warp_runs += (double)c.n / 32.0;
     hc.push_back(b);
   }
+  // Block size: 512 threads (16 warps per SM) when the tile/thread classes
+  // hold more than two waves of warps -- throughput -- else 384 (12 warps,
+  // 170 registers a thread instead of 128: faster per run, which is what a
+  // batch of long-running stragglers waits on).  config->block forces one.
+  int block = config->block == kBatchBlockLarge || config->block == kBatchBlockSmall
+                ? config->block
+                : (warp_runs > 2.0 * sm_count() * (kBatchBlockLarge / 32)
+                     ? kBatchBlockLarge
+                     : kBatchBlockSmall);
+  for (const BatchClass& b : hc)
+    if (b.layout == ZEUS_LAYOUT_CTA &&
+        cta_doubles_rt(b.kind, b.dim, block) * sizeof(double) > 227 * 1024)
+      block = kBatchBlockSmall; // its CTA classes fit at 384 (checked above)
+  size_t smem_cta = 0;
+  for (const BatchClass& b : hc)
+    if (b.layout == ZEUS_LAYOUT_CTA)
+      smem_cta = std::max(smem_cta, cta_doubles_rt(b.kind, b.dim, block));
   // biggest work first: CTA classes by dimension, then the rest by dimension
   std::stable_sort(hc.begin(), hc.end(), [](const BatchClass& a, const BatchClass& b) {
     const int ka = a.layout == ZEUS_LAYOUT_CTA, kb = b.layout == ZEUS_LAYOUT_CTA;
@@ -391,26 +237,9 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
   for (int i = 0; i < n_classes; ++i)
     bt.c[i] = hc[i];
   const size_t smem =
-    sizeof(double) * std::max(smem_cta, smem_tile * (kBatchBlock / 32));
-  rc = cuda_fail(cudaFuncSetAttribute(bfgs_batch_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem),
-                 "batch shared memory attribute");
-  if (rc)
-    return rc;
-  int per_sm = 0;
-  rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                   &per_sm, bfgs_batch_kernel, kBatchBlock, smem),
-                 "batch occupancy");
-  if (rc)
-    return rc;
-  if (per_sm < 1) {
-    set_error("batch kernel does not fit on an SM (%zu bytes of shared memory)",
-              smem);
-    return ZEUS_E_UNSUPPORTED;
-  }
-  bfgs_batch_kernel<<<sm_count() * per_sm, kBatchBlock, smem, st>>>(bt);
-  return cuda_fail(cudaGetLastError(), "batch BFGS launch");
+    sizeof(double) * std::max(smem_cta, smem_tile * (block / 32));
+  return block == kBatchBlockLarge ? launch_batch_512(bt, smem, st)
+                                   : launch_batch_384(bt, smem, st);
 }
 
 } // extern "C"

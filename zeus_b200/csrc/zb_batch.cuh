@@ -2,7 +2,7 @@
 //
 // A class is one (objective, dimension) with its own runs, starts, outputs
 // and stop-early control; classes may have per-instance data (e.g. one toy
-// spectrum per 256 runs).  One block of kBatchBlock threads per SM:
+// spectrum per 256 runs).  One block (512 or 384 threads) per SM:
 //
 //   phase A  the block takes runs of the CTA-layout classes (D > 32) one at
 //            a time from each class's atomic queue, biggest dimension first,
@@ -23,7 +23,9 @@
 
 namespace zb {
 
-  inline constexpr int kBatchBlock = 512;
+  // The kernel is built for two block sizes (one block per SM).
+  inline constexpr int kBatchBlockLarge = 512;
+  inline constexpr int kBatchBlockSmall = 384;
 
   struct BatchClass {
     int kind, dim, layout, tile;
@@ -54,10 +56,11 @@ namespace zb {
   };
 
   // Tile widths compiled into the batch kernel for an objective and
-  // dimension: rows of H of at most 32 doubles per lane (the kernel is
-  // limited to 128 registers per thread by its 512-thread,
-  // one-block-per-SM launch bounds); wider than 2*D only for the objectives
-  // whose cooperative evaluation splits bins or matrix rows.
+  // dimension: at most two rows of H and 32 doubles of it per lane (the
+  // kernel is limited to 128 registers per thread by its 512-thread,
+  // one-block-per-SM launch bounds); at most 4*D lanes (the lanes beyond D
+  // evaluate line-search trials in parallel) except for the objectives whose
+  // cooperative evaluation splits bins or matrix rows.
   __host__ __device__ constexpr unsigned
   batch_widths(int kind, int d)
   {
@@ -68,7 +71,7 @@ namespace zb {
     for (int k = 1; k <= 5; ++k) {
       const int ts = 1 << k;
       const int r = (d + ts - 1) / ts;
-      if (r * d <= 32 && (wide || ts <= 2 * d))
+      if (r <= 2 && r * d <= 32 && (wide || ts <= 4 * d))
         m |= 1u << k;
     }
     return m;
@@ -93,10 +96,13 @@ namespace zb {
     return f;
   }
 
+  int launch_batch_512(const BatchTable& bt, size_t smem, cudaStream_t st);
+  int launch_batch_384(const BatchTable& bt, size_t smem, cudaStream_t st);
+
   __host__ __device__ inline size_t
   batch_tile_buf_doubles(int dim, int ts)
   {
-    return (size_t)(32 / ts) * (4 * dim + ts);
+    return (size_t)(32 / ts) * tile_buf_doubles(dim, ts);
   }
 
 } // namespace zb

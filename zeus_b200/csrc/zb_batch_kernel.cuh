@@ -1,0 +1,224 @@
+// The persistent batch kernel, a template on its block size; each of
+// zb_batch_512.cu and zb_batch_384.cu instantiates one and exports its
+// launcher (the host side, zb_batch.cu, picks one per batch).
+#pragma once
+
+#include "zb_batch.cuh"
+#include "zb_objective_visit.cuh"
+
+namespace zb {
+
+  namespace {
+
+    // Device-side (kind, dim) -> functor, for the dimensions the library is
+    // built for (the same sets as visit_objective).
+    template <class Fn>
+    __device__ __forceinline__ void
+    batch_visit(const BatchClass& c, Fn&& fn)
+    {
+      switch (c.kind) {
+        case ZEUS_OBJ_ROSENBROCK:
+          switch (c.dim) {
+#define ZB_CASE(D)                                                             \
+  case D:                                                                      \
+    fn(zeus::Rosenbrock<D>{});                                                 \
+    return;
+            ZB_ROSENBROCK_DIMS(ZB_CASE)
+#undef ZB_CASE
+          }
+          return;
+        case ZEUS_OBJ_RASTRIGIN:
+          switch (c.dim) {
+#define ZB_CASE(D)                                                             \
+  case D:                                                                      \
+    fn(zeus::Rastrigin<D>{});                                                  \
+    return;
+            ZB_RASTRIGIN_DIMS(ZB_CASE)
+#undef ZB_CASE
+          }
+          return;
+        case ZEUS_OBJ_ACKLEY:
+          switch (c.dim) {
+#define ZB_CASE(D)                                                             \
+  case D:                                                                      \
+    fn(zeus::Ackley<D>{});                                                     \
+    return;
+            ZB_ACKLEY_DIMS(ZB_CASE)
+#undef ZB_CASE
+          }
+          return;
+        case ZEUS_OBJ_GAUSSIAN:
+          switch (c.dim) {
+#define ZB_CASE(D)                                                             \
+  case D: {                                                                    \
+    zeus::Gaussian<D> g;                                                       \
+    g.C = c.data;                                                              \
+    g.symmetric = (c.flags & 1) != 0;                                          \
+    fn(g);                                                                     \
+    return;                                                                    \
+  }
+            ZB_GAUSSIAN_DIMS(ZB_CASE)
+#undef ZB_CASE
+          }
+          return;
+        case ZEUS_OBJ_POISSON_NLL:
+          if (c.dim == 4) {
+            zeus::PoissonNLL p;
+            p.centres = c.data;
+            p.counts = c.idata;
+            p.bins = c.nll_bins;
+            p.nbins = c.ndata;
+            fn(p);
+          }
+          return;
+      }
+    }
+
+    template <class F>
+    __device__ __forceinline__ F
+    instance_for(const F& f, const BatchClass& c, int64_t run)
+    {
+      return c.runs_per_instance > 0 ? with_instance(f, c, run / c.runs_per_instance)
+                                     : f;
+    }
+
+    template <class F, int D, int TS>
+    __device__ __forceinline__ void
+    drain_tile_class(const F& f, const BatchClass& c, const BfgsParams& prm,
+                     double* warp_buf)
+    {
+      auto tile = cg::tiled_partition<TS>(cg::this_thread_block());
+      const int tin = (int)(threadIdx.x & 31) / TS;
+      double* buf = warp_buf + tin * tile_buf_doubles(D, TS);
+      for (;;) {
+        unsigned long long r = 0;
+        if (tile.thread_rank() == 0)
+          r = atomicAdd(c.queue, 1ull);
+        r = tile.shfl(r, 0);
+        if ((int64_t)r >= c.n)
+          break;
+        tile_run<F, D, TS, true>(instance_for(f, c, (int64_t)r), tile, buf, prm,
+                                 c.starts + (int64_t)r * D, (int64_t)r, c.out,
+                                 c.ctl);
+      }
+    }
+
+  } // namespace
+
+  template <int kBlock>
+  __global__ void __launch_bounds__(kBlock, 1)
+    bfgs_batch_kernel(const __grid_constant__ BatchTable bt)
+  {
+    const int ncls = bt.ncls;
+    const BatchClass* classes = bt.c;
+    extern __shared__ __align__(16) double sm[];
+    __shared__ unsigned long long sh_run;
+
+    // phase A: CTA-layout classes, one run per block at a time
+    for (int ci = 0; ci < ncls; ++ci) {
+      const BatchClass c = classes[ci];
+      if (c.layout != ZEUS_LAYOUT_CTA)
+        continue;
+      const BfgsParams prm{c.n, bt.max_iter, c.required, bt.tol, bt.flags};
+      for (;;) {
+        if (threadIdx.x == 0)
+          sh_run = atomicAdd(c.queue, 1ull);
+        __syncthreads();
+        const int64_t r = (int64_t)sh_run;
+        __syncthreads();
+        if (r >= c.n)
+          break;
+        batch_visit(c, [&](auto f) {
+          using F = decltype(f);
+          constexpr int D = (int)F::arity;
+          if constexpr (D >= kBatchCtaMinDim &&
+                        sizeof(double) * cta_smem_doubles<F, D, true>(kBlock) <=
+                          227 * 1024)
+            cta_run<F, D, true, kBlock>(instance_for(f, c, r), sm, prm,
+                                             c.starts + r * D, r, c.out, c.ctl);
+        });
+      }
+    }
+    __syncthreads();
+
+    // phase B: each warp drains the tile / thread classes
+    double* warp_buf = nullptr;
+    {
+      // per-warp buffers follow each other; sized by the host for the
+      // widest class of the batch
+      const int warp = threadIdx.x >> 5;
+      size_t stride = 0;
+      for (int ci = 0; ci < ncls; ++ci)
+        if (classes[ci].layout == ZEUS_LAYOUT_TILE)
+          stride = stride > batch_tile_buf_doubles(classes[ci].dim, classes[ci].tile)
+                     ? stride
+                     : batch_tile_buf_doubles(classes[ci].dim, classes[ci].tile);
+      warp_buf = sm + (size_t)warp * stride;
+    }
+    for (int ci = 0; ci < ncls; ++ci) {
+      const BatchClass c = classes[ci];
+      if (c.layout == ZEUS_LAYOUT_CTA)
+        continue;
+      const BfgsParams prm{c.n, bt.max_iter, c.required, bt.tol, bt.flags};
+      batch_visit(c, [&](auto f) {
+        using F = decltype(f);
+        constexpr int D = (int)F::arity;
+        if (c.layout == ZEUS_LAYOUT_THREAD) {
+          if constexpr (D <= kBatchThreadMaxDim) {
+            for (;;) {
+              const int64_t r = (int64_t)atomicAdd(c.queue, 1ull);
+              if (r >= c.n)
+                break;
+              thread_run<F, D, true>(instance_for(f, c, r), prm,
+                                     c.starts + r * D, r, c.out, c.ctl);
+            }
+          }
+        } else if constexpr (D < kBatchCtaMinDim) {
+          constexpr unsigned W = batch_widths(F::kind, D);
+          switch (c.tile) {
+#define ZB_TS(K)                                                               \
+  case (1 << K):                                                               \
+    if constexpr ((W >> K) & 1u)                                               \
+      drain_tile_class<F, D, (1 << K)>(f, c, prm, warp_buf);                   \
+    break;
+            ZB_TS(1)
+            ZB_TS(2)
+            ZB_TS(3)
+            ZB_TS(4)
+            ZB_TS(5)
+#undef ZB_TS
+          }
+        }
+      });
+      __syncwarp();
+    }
+  }
+
+
+  // Sets the shared-memory attribute, sizes the grid to the SMs and launches.
+  template <int kBlock>
+  int
+  launch_batch_kernel(const BatchTable& bt, size_t smem, cudaStream_t st)
+  {
+    auto kern = bfgs_batch_kernel<kBlock>;
+    int rc = cuda_fail(cudaFuncSetAttribute(
+                         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                       "batch shared memory attribute");
+    if (rc)
+      return rc;
+    int per_sm = 0;
+    rc = cuda_fail(
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem),
+      "batch occupancy");
+    if (rc)
+      return rc;
+    if (per_sm < 1) {
+      set_error("batch kernel does not fit on an SM (%zu bytes of shared memory)",
+                smem);
+      return ZEUS_E_UNSUPPORTED;
+    }
+    kern<<<sm_count() * per_sm, kBlock, smem, st>>>(bt);
+    return cuda_fail(cudaGetLastError(), "batch BFGS launch");
+  }
+
+} // namespace zb

@@ -82,18 +82,59 @@ namespace zb {
     }
   }
 
+  template <class F, class G>
+  concept HasGradientCoop =
+    requires(const F& f, const G& g, const double* x, double* gr) {
+      f.gradient_coop(g, x, gr);
+    };
+
+  // g = grad f(x) without f(x): objectives with a reduction-free gradient
+  // skip the value's reduction.
+  template <class F, int D, bool Adjoint, class G>
+  __device__ __forceinline__ void
+  coop_gradient_only(const F& f, const G& grp, const double* x, double* g)
+  {
+    if constexpr (Adjoint && HasGradientCoop<F, G>)
+      f.gradient_coop(grp, x, g);
+    else
+      (void)coop_gradient<F, D, Adjoint>(f, grp, x, g);
+  }
+
   // ---------------------------------------------------------------- tile
   inline constexpr int kTileBlock = 128;
 
+  // Per-tile shared memory (doubles): trial point xs[D] | gradient gs[D] |
+  // {s, w, y, g_next}[D] | {x, p}[D] | scratch TS.
+  __host__ __device__ constexpr int
+  tile_buf_doubles(int d, int ts)
+  {
+    return 8 * d + ts;
+  }
   template <int D, int TS>
   constexpr int
   tile_smem_doubles()
   {
-    return 4 * D + TS; // xs, gs, b1, b2, scratch
+    return tile_buf_doubles(D, TS);
   }
 
+  // f(x + a p) evaluated by one thread from interleaved {x_i, p_i}.
+  template <class F>
+  concept HasValueLine = requires(const F& f, const double2* xp, double a) {
+    { f.value_line(xp, a) } -> std::convertible_to<double>;
+  };
+
   // One run on a tile: `buf` is the tile's tile_smem_doubles<D, TS>()
-  // doubles of shared memory; start x0[D]; results to slot `run` of `out`.
+  // doubles of shared memory (16-byte aligned); start x0[D]; results to
+  // slot `run` of `out`.
+  //
+  // Line search: trial 0 on the whole tile (cooperative value), then, for
+  // objectives with value_line, the remaining trials lane-per-trial, TS at
+  // a time, the first passing one found by a ballot (for D <= 8 every trial
+  // goes lane-per-trial).  Then one pass over the H rows in registers
+  // applies the previous iteration's deferred update H += s w^T + w s^T and
+  // forms u = H y and h = H g_next together, and one butterfly reduction of
+  // {s.y, y.u, u.g, s.g, g.h, g.g, stop} gives every scalar:
+  //   p+ = -(h + s (w.g) + w (s.g)),  g.p+ = -(g.h + 2 (s.g)(w.g)).
   template <class F, int D, int TS, bool Adjoint>
   __device__ __forceinline__ void
   tile_run(const F& f, cg::thread_block_tile<TS> tile, double* buf,
@@ -101,133 +142,231 @@ namespace zb {
            const RunOut& out, Control* ctl)
   {
     constexpr int R = (D + TS - 1) / TS;
+    constexpr bool kLine = HasValueLine<F>;
+    constexpr bool kCoopFirst = !kLine || D > 8;
     const int lane = (int)tile.thread_rank();
     double* xs = buf;
     double* gs = xs + D;
-    double* b1 = gs + D;
-    double* b2 = b1 + D;
-    TileGroup<TS> grp(tile, b2 + D);
+    double* quad = gs + D; // [D][4]: s, w, y, g_next
+    double* xp = quad + 4 * D; // [D][2]: x, p
+    TileGroup<TS> grp(tile, xp + 2 * D);
 
-    double x[R], g[R], p[R], H[R][D];
+    double x[R], g[R], p[R], sp[R], wp[R], H[R][D];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int i = lane + r * TS;
       x[r] = i < D ? x0[i] : 0.0;
       if (i < D)
         xs[i] = x[r];
+      sp[r] = 0.0;
+      wp[r] = 0.0;
 #pragma unroll
       for (int j = 0; j < D; ++j)
         H[r][j] = (i == j) ? 1.0 : 0.0;
     }
     grp.sync();
     double best = coop_value<F, D>(f, grp, xs);
-    coop_gradient<F, D, Adjoint>(f, grp, xs, gs);
+    coop_gradient_only<F, D, Adjoint>(f, grp, xs, gs);
     grp.sync();
+    double ddir;
+    bool stop;
+    {
+      double v[2] = {0.0, lane == 0 ? (double)load_stop(ctl) : 0.0};
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int i = lane + r * TS;
-      g[r] = i < D ? gs[i] : 0.0;
-      p[r] = -g[r];
+      for (int r = 0; r < R; ++r) {
+        const int i = lane + r * TS;
+        g[r] = i < D ? gs[i] : 0.0;
+        p[r] = -g[r];
+        v[0] = fma(g[r], p[r], v[0]);
+      }
+      grp.template sum<2>(v);
+      ddir = v[0];
+      stop = v[1] != 0.0;
     }
+    bool pend = false;
     long long n_eval = 1, n_grad = 1;
     int status = kUnset, iter, executed = -1;
     double fout = best, gout = 0.0;
 
     for (iter = 0; iter < prm.max_iter; ++iter) {
-      const int stop = grp.bcast(lane == 0 ? load_stop(ctl) : 0, 0);
       if (stop) {
         status = kStopped;
         break;
       }
-      double dd = 0.0;
-#pragma unroll
-      for (int r = 0; r < R; ++r)
-        dd = fma(g[r], p[r], dd);
-      const double ddir = grp.sum(dd);
-      double xn[R], alpha = 1.0, fnew = 0.0;
-      bool ok = false;
-      for (int k = 0; k <= kLineSearchTrials; ++k) {
+      const int stop_now = lane == 0 ? load_stop(ctl) : 0; // consumed below
+      // ---- line search: alpha_k = 2^-k, first k in 0..19 that passes,
+      // else alpha = 2^-20 (utils.cuh:376-412)
+      int found = -1;
+      double fnew = 0.0;
+      if constexpr (kCoopFirst) {
         grp.sync(); // earlier readers of xs are done
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           const int i = lane + r * TS;
-          xn[r] = fma(alpha, p[r], x[r]);
           if (i < D)
-            xs[i] = xn[r];
+            xs[i] = fma(1.0, p[r], x[r]);
         }
         grp.sync();
-        const double f1 = coop_value<F, D>(f, grp, xs);
-        ++n_eval;
-        if (k == kLineSearchTrials) { // all 20 failed: alpha = 2^-20
-          fnew = f1;
-          break;
+        const double f0 = coop_value<F, D>(f, grp, xs);
+        if (f0 <= best + kArmijoC1 * ddir && f0 < best) {
+          found = 0;
+          fnew = f0;
         }
-        if (f1 <= best + kArmijoC1 * alpha * ddir && f1 < best) {
-          ok = true;
-          fnew = f1;
-          break;
-        }
-        alpha *= 0.5;
       }
-      (void)ok;
+      if (found < 0) {
+        constexpr int k0 = kCoopFirst ? 1 : 0;
+        if constexpr (kLine) {
+          grp.sync(); // earlier readers of xp are done
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const int i = lane + r * TS;
+            if (i < D)
+              *reinterpret_cast<double2*>(xp + 2 * i) = make_double2(x[r], p[r]);
+          }
+          grp.sync();
+          for (int base = k0; found < 0; base += TS) {
+            const int k = base + lane;
+            double fk = 0.0;
+            bool pass = false;
+            if (k <= kLineSearchTrials) {
+              const double ak = pow2neg(k);
+              fk = f.value_line(reinterpret_cast<const double2*>(xp), ak);
+              pass = k == kLineSearchTrials ||
+                     (fk <= best + kArmijoC1 * ak * ddir && fk < best);
+            }
+            const unsigned m = tile.ballot(pass);
+            if (m) {
+              const int wl = __ffs(m) - 1;
+              found = base + wl;
+              fnew = tile.shfl(fk, wl);
+            }
+          }
+        } else {
+          double a = pow2neg(k0);
+          for (int k = k0; k <= kLineSearchTrials; ++k, a *= 0.5) {
+            grp.sync();
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              const int i = lane + r * TS;
+              if (i < D)
+                xs[i] = fma(a, p[r], x[r]);
+            }
+            grp.sync();
+            const double f1 = coop_value<F, D>(f, grp, xs);
+            if (k == kLineSearchTrials ||
+                (f1 <= best + kArmijoC1 * a * ddir && f1 < best)) {
+              found = k;
+              fnew = f1;
+              break;
+            }
+          }
+        }
+      }
+      n_eval += found + 1;
+      const double alpha = pow2neg(found);
+      double xn[R];
+      grp.sync(); // readers of xs are done
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = lane + r * TS;
+        xn[r] = fma(alpha, p[r], x[r]);
+        if (i < D)
+          xs[i] = xn[r];
+      }
       grp.sync();
-      coop_gradient<F, D, Adjoint>(f, grp, xs, gs);
+      coop_gradient_only<F, D, Adjoint>(f, grp, xs, gs);
       ++n_grad;
       grp.sync();
-      double gn[R], s[R], y[R];
-      double sy_part = 0.0;
+      const bool take = fnew < best;
+      double gn[R], s[R], y[R], gx[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const int i = lane + r * TS;
         gn[r] = i < D ? gs[i] : 0.0;
         s[r] = xn[r] - x[r];
         y[r] = gn[r] - g[r];
-        sy_part = fma(s[r], y[r], sy_part);
+        gx[r] = take ? gn[r] : g[r];
+        if (i < D)
+          *reinterpret_cast<double2*>(quad + 4 * i + 2) = make_double2(y[r], gx[r]);
       }
-      const double sy = grp.sum(sy_part);
-      const bool skipped = fabs(sy) < kMinCurvature;
-      if (!skipped) {
-        const double rho = 1.0 / sy;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int i = lane + r * TS;
-          if (i < D)
-            b1[i] = y[r];
-        }
-        grp.sync();
-        double u[R], yu_part = 0.0;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-          double a = 0.0;
-#pragma unroll
-          for (int j = 0; j < D; ++j)
-            a = fma(H[r][j], b1[j], a);
-          u[r] = a;
-          yu_part = fma(y[r], a, yu_part);
-        }
-        const double yu = grp.sum(yu_part);
-        const double hb = 0.5 * rho * fma(rho, yu, 1.0);
-        double w[R];
+      grp.sync();
+      // ---- one pass: deferred update, u = H y, h = H g_next (even and odd
+      // columns in separate sums: half the chain of dependent FMAs)
+      double u[R], hh[R];
+      {
+        double ua[R][2], ha[R][2];
 #pragma unroll
         for (int r = 0; r < R; ++r)
-          w[r] = fma(hb, s[r], -rho * u[r]);
-        grp.sync(); // b1 (= y) fully read
+          ua[r][0] = ua[r][1] = ha[r][0] = ha[r][1] = 0.0;
+        if (pend) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-          const int i = lane + r * TS;
-          if (i < D) {
-            b1[i] = s[r];
-            b2[i] = w[r];
+          for (int j = 0; j < D; ++j) {
+            const double2 sw = *reinterpret_cast<const double2*>(quad + 4 * j);
+            const double2 yg = *reinterpret_cast<const double2*>(quad + 4 * j + 2);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              H[r][j] += __dadd_rn(__dmul_rn(sp[r], sw.y), __dmul_rn(wp[r], sw.x));
+              ua[r][j & 1] = fma(H[r][j], yg.x, ua[r][j & 1]);
+              ha[r][j & 1] = fma(H[r][j], yg.y, ha[r][j & 1]);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < D; ++j) {
+            const double2 yg = *reinterpret_cast<const double2*>(quad + 4 * j + 2);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+              ua[r][j & 1] = fma(H[r][j], yg.x, ua[r][j & 1]);
+              ha[r][j & 1] = fma(H[r][j], yg.y, ha[r][j & 1]);
+            }
           }
         }
-        grp.sync();
 #pragma unroll
-        for (int r = 0; r < R; ++r)
-#pragma unroll
-          for (int j = 0; j < D; ++j)
-            H[r][j] += __dadd_rn(__dmul_rn(s[r], b2[j]), __dmul_rn(w[r], b1[j]));
+        for (int r = 0; r < R; ++r) {
+          u[r] = ua[r][0] + ua[r][1];
+          hh[r] = ha[r][0] + ha[r][1];
+        }
       }
-      const bool take = fnew < best;
+      double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, (double)stop_now};
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = lane + r * TS;
+        if (i < D) {
+          v[0] = fma(s[r], y[r], v[0]);
+          v[1] = fma(y[r], u[r], v[1]);
+          v[2] = fma(u[r], gx[r], v[2]);
+          v[3] = fma(s[r], gx[r], v[3]);
+          v[4] = fma(gx[r], hh[r], v[4]);
+          v[5] = fma(gx[r], gx[r], v[5]);
+        }
+      }
+      grp.template sum<7>(v);
+      const bool skipped = fabs(v[0]) < kMinCurvature;
+      const double sg = v[3], gh = v[4];
+      double rho = 0.0, hb = 0.0, wg = 0.0;
+      if (!skipped) {
+        rho = 1.0 / v[0];
+        hb = 0.5 * rho * fma(rho, v[1], 1.0);
+        wg = hb * sg - rho * v[2];
+      }
+      grp.sync(); // every lane's pass has read quad
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int i = lane + r * TS;
+        if (!skipped) {
+          const double w = fma(hb, s[r], -rho * u[r]);
+          p[r] = -(hh[r] + s[r] * wg + w * sg);
+          sp[r] = s[r];
+          wp[r] = w;
+          if (i < D)
+            *reinterpret_cast<double2*>(quad + 4 * i) = make_double2(s[r], w);
+        } else {
+          p[r] = -hh[r];
+        }
+      }
+      pend = !skipped;
+      ddir = skipped ? -gh : -(gh + 2.0 * sg * wg);
+      stop = v[6] != 0.0;
       if (take) {
         best = fnew;
 #pragma unroll
@@ -236,11 +375,7 @@ namespace zb {
           g[r] = gn[r];
         }
       }
-      double gg = 0.0;
-#pragma unroll
-      for (int r = 0; r < R; ++r)
-        gg = fma(g[r], g[r], gg);
-      const double gnrm = sqrt(grp.sum(gg));
+      const double gnrm = sqrt(v[5]);
       if (!isfinite(gnrm) || !isfinite(fnew)) {
         status = kNonFinite;
         fout = fnew;
@@ -259,22 +394,6 @@ namespace zb {
         executed = iter + 1;
         iter = prm.max_iter;
         break;
-      }
-      grp.sync(); // b1 / b2 fully read
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        const int i = lane + r * TS;
-        if (i < D)
-          b1[i] = g[r];
-      }
-      grp.sync();
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        double a = 0.0;
-#pragma unroll
-        for (int j = 0; j < D; ++j)
-          a = fma(H[r][j], b1[j], a);
-        p[r] = -a;
       }
     }
     if (status == kUnset || status == kStopped) {
@@ -308,6 +427,7 @@ namespace zb {
         out.counters[3 * run + 2] = n_grad;
       }
     }
+    grp.sync();
   }
 
   template <class F, int D, int TS, bool Adjoint>
@@ -316,7 +436,7 @@ namespace zb {
                      RunOut out, Control* ctl)
   {
     constexpr int TPB = kTileBlock / TS;
-    extern __shared__ double sm[];
+    extern __shared__ __align__(16) double sm[];
     auto tile = cg::tiled_partition<TS>(cg::this_thread_block());
     const int tslot = threadIdx.x / TS;
     const int64_t run = (int64_t)blockIdx.x * TPB + tslot;
@@ -327,16 +447,75 @@ namespace zb {
   }
 
   // ---------------------------------------------------------------- CTA
-  // Shared-memory layout (doubles): H[D*D] | 11 vectors of D | partial sums
-  // 2*Q*D | reduction buffers kCtaRedDoubles | scratch blockDim | trial
-  // values 2*32 | flags 4 | (warp trials) one trial point per warp,
-  // (blockDim/32)*D.
+  // One run on the whole thread block, H in shared memory (D x D doubles,
+  // exactly symmetric).  An iteration meets at four block barriers:
+  //
+  //   1. line search: warp w evaluates trial k = r0 + w of a round on its own
+  //      copy of the trial point (shuffle reductions only); one barrier
+  //      publishes the round's values and every warp finds the first passing
+  //      trial with one ballot.  (Objectives whose trials carry the gradient
+  //      -- the Gaussian's C x -- evaluate trials one at a time on the whole
+  //      block.)
+  //   2. gradient at the accepted point.
+  //   3. one sweep over H: it applies the previous iteration's deferred
+  //      rank-2 update H += s w^T + w s^T in place and forms the column
+  //      partial sums of u = H y and h = H g_next (C = 2 columns per thread
+  //      with 16-byte accesses, Q = blockDim / (D / C) groups of rows).
+  //   4. one block reduction of {s.y, y.u, u.g, s.g, g.h, g.g, stop}; every
+  //      scalar of the update follows from it:
+  //        w = hb s - rho u,  w.g = hb (s.g) - rho (u.g),
+  //        p+ = -H+ g = -(h + s (w.g) + w (s.g)),  g.p+ = -(g.h + 2 (s.g)(w.g)).
+  //
+  // x, p and the accepted point stay in registers, replicated in every warp
+  // (lane l holds coordinates l, l+32, ...): each warp forms the same p+
+  // from u and h in shared memory, so no barrier publishes p.
+  template <int D>
+  struct CtaShape {
+    static constexpr int C = (D % 2 == 0) ? 2 : 1; // sweep columns per thread
+    static constexpr int NCOL = D / C;
+    static constexpr int RV = (D + 31) / 32; // coordinates per lane
+  };
+
+  __host__ __device__ constexpr int
+  cta_sweep_q(int d, int block)
+  {
+    const int ncol = (d % 2 == 0) ? d / 2 : d;
+    return block >= ncol ? block / ncol : 1;
+  }
+
+  // Shared-memory layout (doubles): H[D*D, rounded up to even] | {s,w}[D] |
+  // g[2][D] | u[D] | h[D] | partial sums 2*Q*D | trial point D | (group
+  // trials) one trial point per trial group | trial values 2*32 |
+  // reductions | scratch blockDim.
+  __host__ __device__ constexpr size_t
+  cta_smem_base_doubles(int d, int block)
+  {
+    const int q = cta_sweep_q(d, block);
+    return (((size_t)d * d + 1) & ~(size_t)1) + 6 * (size_t)d +
+           2 * (size_t)q * d + (size_t)d + 64 + kCtaRedDoubles + block;
+  }
+
+  // Lanes per line-search trial group: the widest of 32, 16, 8 that gives
+  // the block at least 21 groups (every trial of a line search in one
+  // round), narrower only while the trial points fit in shared memory.
+  __host__ __device__ constexpr int
+  cta_trial_width(int d, int block)
+  {
+    const int nw = block / 32;
+    const size_t cap = 227 * 1024 / sizeof(double);
+    int st = nw >= 21 ? 32 : 2 * nw >= 21 ? 16 : 8;
+    while (st < 32 &&
+           cta_smem_base_doubles(d, block) + (size_t)nw * (32 / st) * d > cap)
+      st *= 2;
+    return st;
+  }
+
   __host__ __device__ constexpr size_t
   cta_smem_doubles_rt(int d, int block, bool warp_trials)
   {
-    const int q = block >= d ? block / d : 1;
-    return (size_t)d * d + 11 * d + 2 * q * d + kCtaRedDoubles + block + 64 + 4 +
-           (warp_trials ? (size_t)(block / 32) * d : 0);
+    return cta_smem_base_doubles(d, block) +
+           (warp_trials ? (size_t)(block / 32) * (32 / cta_trial_width(d, block)) * d
+                        : 0);
   }
 
   // Line-search trials are evaluated one per warp, all warps at once, unless
@@ -355,230 +534,325 @@ namespace zb {
     return cta_smem_doubles_rt(D, block, cta_warp_trials<F, Adjoint>());
   }
 
+  __device__ __forceinline__ double
+  warp_allsum(double v)
+  {
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1)
+      v += __shfl_xor_sync(0xffffffffu, v, m);
+    return v;
+  }
+
   // One run on the whole block (blockDim.x == kBlock): `sm` holds
-  // cta_smem_doubles<D>(kBlock) doubles; start x0[D]; results to slot `run`.
+  // cta_smem_doubles<F, D, Adjoint>(kBlock) doubles, 16-byte aligned; start
+  // x0[D]; results to slot `run`.
   template <class F, int D, bool Adjoint, int kBlock>
   __device__ __forceinline__ void
   cta_run(const F& f, double* sm, const BfgsParams& prm,
           const double* __restrict__ x0, int64_t run, const RunOut& out,
           Control* ctl)
   {
-    constexpr int Q = kBlock >= D ? kBlock / D : 1;
+    using S = CtaShape<D>;
+    constexpr int C = S::C, NCOL = S::NCOL, RV = S::RV;
+    constexpr int Q = cta_sweep_q(D, kBlock);
     constexpr bool kTrialGrad = Adjoint && TrialsWithGradient<F>;
     constexpr bool kWarpTrials = cta_warp_trials<F, Adjoint>();
     constexpr int NW = kBlock / 32;
+    constexpr int ST = cta_trial_width(D, kBlock); // lanes per trial group
+    constexpr int TPW = 32 / ST;                   // trial groups per warp
+    constexpr int NG = NW * TPW;
+    static_assert(kBlock % 32 == 0 && NCOL <= kBlock, "block too small for D");
+    static_assert(NG <= 32, "one ballot judges a round");
+    static_assert(RV <= NW, "one warp per 32 coordinates at least");
     double* H = sm;
-    double* x = H + D * D;
-    double* g = x + D;
-    double* p = g + D;
-    double* xn = p + D;
-    double* gn = xn + D;
-    double* s = gn + D;
-    double* y = s + D;
-    double* w = y + D;
-    double* u = w + D;
+    double* SW = H + ((D * D + 1) & ~1); // {s_i, w_i} of the deferred update (16 B)
+    double* gb = SW + 2 * D;    // two gradient slots of D
+    double* u = gb + 2 * D;
     double* h = u + D;
-    double* gt = h + D; // gradient computed at line-search trials
-    double* partU = gt + D;
+    double* partU = h + D;
     double* partH = partU + Q * D;
-    double* red = partH + Q * D;
+    double* xt = partH + Q * D; // block trial point / start
+    double* trial_x = xt + D;   // NG x D when kWarpTrials
+    double* tf = trial_x + (kWarpTrials ? NG * D : 0); // 2 x 32
+    double* red = tf + 64;
     double* scratch = red + kCtaRedDoubles;
-    double* trial_f = scratch + kBlock; // 2 x 32: alternate rounds
-    double* trial_x = trial_f + 64 + 4; // NW x D when kWarpTrials
     CtaGroup grp{red, scratch};
-    const int t = threadIdx.x;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
 
+    double xr[RV], pr[RV], xnr[RV];
+#pragma unroll
+    for (int r = 0; r < RV; ++r) {
+      const int i = lane + 32 * r;
+      xr[r] = i < D ? x0[i] : 0.0;
+      pr[r] = 0.0;
+      xnr[r] = 0.0;
+    }
     for (int i = t; i < D; i += kBlock)
-      x[i] = x0[i];
+      xt[i] = x0[i];
     for (int e = t; e < D * D; e += kBlock)
       H[e] = (e / D == e % D) ? 1.0 : 0.0;
     __syncthreads();
+    int cur = 0; // current gradient in slot cur, the new one goes to cur ^ 1
     double best;
     if constexpr (kTrialGrad)
-      best = coop_gradient<F, D, Adjoint>(f, grp, x, g);
+      best = coop_gradient<F, D, Adjoint>(f, grp, xt, gb);
     else {
-      best = coop_value<F, D>(f, grp, x);
-      coop_gradient<F, D, Adjoint>(f, grp, x, g);
+      best = coop_value<F, D>(f, grp, xt);
+      coop_gradient_only<F, D, Adjoint>(f, grp, xt, gb);
     }
     __syncthreads();
     double ddir;
     bool stop;
     {
       double v[2] = {0.0, t == 0 ? (double)load_stop(ctl) : 0.0};
-      for (int i = t; i < D; i += kBlock) {
-        p[i] = -g[i];
-        v[0] = fma(g[i], p[i], v[0]);
-      }
+      if (t < D)
+        v[0] = fma(gb[t], -gb[t], 0.0);
       grp.template sum<2>(v);
       ddir = v[0];
       stop = v[1] != 0.0;
+#pragma unroll
+      for (int r = 0; r < RV; ++r) {
+        const int i = lane + 32 * r;
+        if (i < D)
+          pr[r] = -gb[i];
+      }
     }
     long long n_eval = 1, n_grad = 1;
     int status = kUnset, iter, executed = -1;
     double fout = best, gout = 0.0;
+    bool pend = false; // SW holds an update not yet applied to H
 
     for (iter = 0; iter < prm.max_iter; ++iter) {
       if (stop) {
         status = kStopped;
         break;
       }
+      // this iteration's read of the stop flag, issued now and consumed at
+      // the reduction, so its latency hides behind the line search
+      const int stop_now = t == 0 ? load_stop(ctl) : 0;
       // ---- line search: alpha_k = 2^-k, first k in 0..19 that passes,
       // else alpha = 2^-20 (utils.cuh:376-412)
-      double fnew = 0.0;
-      bool have_grad = false;
+      double fnew = 0.0, alpha = 1.0;
+      const double* xn_s = xt; // accepted point in shared memory
       if constexpr (kWarpTrials) {
-        // warp w evaluates trial k = r0 + w of each round on its own copy of
-        // the trial point (shuffle reductions, no block barrier); one
-        // barrier per round publishes the values, which every thread scans
-        // in trial order
-        const int warp = t >> 5, lane = t & 31;
-        double* wx = trial_x + warp * D;
-        const TileGroup<32> wg(cg::tiled_partition<32>(cg::this_thread_block()),
-                               scratch + warp * 32);
-        int found = -1, round = 0;
-        double alpha = 0.0;
-        for (int r0 = 0; found < 0; r0 += NW, ++round) {
-          const int k = r0 + warp;
-          double f1 = 0.0;
-          if (k <= kLineSearchTrials) {
-            const double ak = ldexp(1.0, -k);
-            for (int i = lane; i < D; i += 32)
-              wx[i] = fma(ak, p[i], x[i]);
-            __syncwarp();
-            f1 = coop_value<F, D>(f, wg, wx);
-            __syncwarp();
-          }
-          double* tf = trial_f + (round & 1) * 32;
-          if (lane == 0)
-            tf[warp] = f1;
-          __syncthreads();
-          for (int w = 0; w < NW; ++w) {
-            const int kk = r0 + w;
-            if (kk > kLineSearchTrials)
-              break;
-            const double fk = tf[w], ak = ldexp(1.0, -kk);
-            if (kk == kLineSearchTrials ||
-                (fk <= best + kArmijoC1 * ak * ddir && fk < best)) {
-              found = kk;
-              fnew = fk;
-              alpha = ak;
-              break;
+        // trial group g = warp * TPW + sub (ST lanes) evaluates trial
+        // k = r0 + g of each round on its own copy of the trial point; the
+        // warp writes its TPW trial points from its registers
+        double* wx = trial_x + warp * TPW * D;
+        const int sub = lane / ST;
+        const TileGroup<ST> sg(cg::tiled_partition<ST>(cg::this_thread_block()),
+                               scratch + warp * 32 + sub * ST);
+        int found = -1;
+        for (int r0 = 0, round = 0; found < 0; r0 += NG, ++round) {
+#pragma unroll
+          for (int q = 0; q < TPW; ++q) {
+            const int k = r0 + warp * TPW + q;
+            if (k <= kLineSearchTrials) {
+              const double ak = pow2neg(k);
+#pragma unroll
+              for (int r = 0; r < RV; ++r) {
+                const int i = lane + 32 * r;
+                if (i < D)
+                  wx[q * D + i] = fma(ak, pr[r], xr[r]);
+              }
             }
+          }
+          __syncwarp();
+          const int k = r0 + warp * TPW + sub;
+          double f1 = 0.0;
+          if (k <= kLineSearchTrials) // uniform within the group
+            f1 = coop_value<F, D>(f, sg, wx + sub * D);
+          double* tfr = tf + (round & 1) * 32;
+          if (sg.rank() == 0)
+            tfr[warp * TPW + sub] = f1;
+          __syncthreads();
+          // lane l judges trial r0 + l; the lowest passing trial wins
+          const int kk = r0 + lane;
+          bool pass = false;
+          double fk = 0.0;
+          if (lane < NG && kk <= kLineSearchTrials) {
+            fk = tfr[lane];
+            const double ak = pow2neg(kk);
+            pass = kk == kLineSearchTrials ||
+                   (fk <= best + kArmijoC1 * ak * ddir && fk < best);
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, pass);
+          if (m) {
+            const int wl = __ffs(m) - 1;
+            found = r0 + wl;
+            fnew = __shfl_sync(0xffffffffu, fk, wl);
+            alpha = pow2neg(found);
+            xn_s = trial_x + wl * D;
           }
         }
         n_eval += found + 1;
-        for (int i = t; i < D; i += kBlock)
-          xn[i] = fma(alpha, p[i], x[i]);
       } else {
-        double alpha = 1.0;
+        double* gt = gb + (cur ^ 1) * D;
         for (int k = 0; k <= kLineSearchTrials; ++k) {
-          for (int i = t; i < D; i += kBlock)
-            xn[i] = fma(alpha, p[i], x[i]);
+          if (warp == 0) {
+#pragma unroll
+            for (int r = 0; r < RV; ++r) {
+              const int i = lane + 32 * r;
+              if (i < D)
+                xt[i] = fma(alpha, pr[r], xr[r]);
+            }
+          }
           __syncthreads();
           double f1;
           if constexpr (kTrialGrad)
-            f1 = coop_gradient<F, D, Adjoint>(f, grp, xn, gt);
+            f1 = coop_gradient<F, D, Adjoint>(f, grp, xt, gt);
           else
-            f1 = coop_value<F, D>(f, grp, xn);
+            f1 = coop_value<F, D>(f, grp, xt);
           ++n_eval;
           if (k == kLineSearchTrials ||
               (f1 <= best + kArmijoC1 * alpha * ddir && f1 < best)) {
             fnew = f1;
-            have_grad = kTrialGrad;
             break;
           }
           alpha *= 0.5;
-          __syncthreads(); // xn fully read before the next trial writes it
+          __syncthreads(); // xt fully read before the next trial writes it
         }
       }
-      __syncthreads();
-      if (have_grad) {
-        for (int i = t; i < D; i += kBlock)
-          gn[i] = gt[i];
-      } else {
-        coop_gradient<F, D, Adjoint>(f, grp, xn, gn);
-      }
+#pragma unroll
+      for (int r = 0; r < RV; ++r) // the accepted point, bit for bit
+        xnr[r] = fma(alpha, pr[r], xr[r]);
+      double* gn = gb + (cur ^ 1) * D;
+      const double* g = gb + cur * D;
+      if constexpr (!kTrialGrad)
+        coop_gradient_only<F, D, Adjoint>(f, grp, xn_s, gn);
       ++n_grad;
       __syncthreads();
       const bool take = fnew < best;
-      double sy_part = 0.0;
-      for (int i = t; i < D; i += kBlock) {
-        s[i] = xn[i] - x[i];
-        y[i] = gn[i] - g[i];
-        sy_part = fma(s[i], y[i], sy_part);
-      }
-      const double sy = grp.sum(sy_part); // (its barriers publish s, y)
-      const bool skipped = fabs(sy) < kMinCurvature;
-      const double* gnext = take ? gn : g;
-      // sweep 1: u = H y (if updating) and h = H g_next, by columns
+      const double* gx = take ? gn : g; // the gradient p+ is formed for
+
+      // ---- sweep: deferred update + column partial sums of H y and H g_next
       {
-        const int i = t % D, q = t / D;
-        if (q < Q && t < Q * D) {
-          double au = 0.0, ah = 0.0;
-          for (int m = q; m < D; m += Q) {
-            const double hv = H[m * D + i];
-            ah = fma(hv, gnext[m], ah);
-            if (!skipped)
-              au = fma(hv, y[m], au);
+        const int c = t % NCOL, q = t / NCOL;
+        if (q < Q) {
+          const int i0 = C * c;
+          double si[C], wi[C], au[C], ah[C];
+#pragma unroll
+          for (int j = 0; j < C; ++j) {
+            si[j] = pend ? SW[2 * (i0 + j)] : 0.0;
+            wi[j] = pend ? SW[2 * (i0 + j) + 1] : 0.0;
+            au[j] = 0.0;
+            ah[j] = 0.0;
           }
-          partU[q * D + i] = au;
-          partH[q * D + i] = ah;
+          if (pend) {
+#pragma unroll 4
+            for (int m = q; m < D; m += Q) {
+              const double2 sw = *reinterpret_cast<const double2*>(SW + 2 * m);
+              const double gm = gx[m], ym = gn[m] - g[m];
+              double* row = H + m * D + i0;
+              double hv[C];
+              if constexpr (C == 2) {
+                const double2 v2 = *reinterpret_cast<const double2*>(row);
+                hv[0] = v2.x;
+                hv[1] = v2.y;
+              } else {
+                hv[0] = row[0];
+              }
+#pragma unroll
+              for (int j = 0; j < C; ++j)
+                hv[j] += __dadd_rn(__dmul_rn(sw.x, wi[j]), __dmul_rn(sw.y, si[j]));
+              if constexpr (C == 2)
+                *reinterpret_cast<double2*>(row) = make_double2(hv[0], hv[1]);
+              else
+                row[0] = hv[0];
+#pragma unroll
+              for (int j = 0; j < C; ++j) {
+                ah[j] = fma(hv[j], gm, ah[j]);
+                au[j] = fma(hv[j], ym, au[j]);
+              }
+            }
+          } else {
+#pragma unroll 4
+            for (int m = q; m < D; m += Q) {
+              const double gm = gx[m], ym = gn[m] - g[m];
+              const double* row = H + m * D + i0;
+              double hv[C];
+              if constexpr (C == 2) {
+                const double2 v2 = *reinterpret_cast<const double2*>(row);
+                hv[0] = v2.x;
+                hv[1] = v2.y;
+              } else {
+                hv[0] = row[0];
+              }
+#pragma unroll
+              for (int j = 0; j < C; ++j) {
+                ah[j] = fma(hv[j], gm, ah[j]);
+                au[j] = fma(hv[j], ym, au[j]);
+              }
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < C; ++j) {
+            partU[q * D + i0 + j] = au[j];
+            partH[q * D + i0 + j] = ah[j];
+          }
         }
       }
       __syncthreads();
-      double yu_part = 0.0;
-      for (int i = t; i < D; i += kBlock) {
-        double au = 0.0, ah = 0.0;
+
+      // ---- one reduction for every scalar of the update and the checks
+      double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      if (t < D) { // coordinate t is slot r = warp of this lane
+        double uu = 0.0, hh = 0.0;
+#pragma unroll 4
         for (int q = 0; q < Q; ++q) {
-          au += partU[q * D + i];
-          ah += partH[q * D + i];
+          uu += partU[q * D + t];
+          hh += partH[q * D + t];
         }
-        u[i] = au;
-        h[i] = ah;
-        yu_part = fma(y[i], au, yu_part);
+        u[t] = uu;
+        h[t] = hh;
+        double st = 0.0;
+#pragma unroll
+        for (int r = 0; r < RV; ++r)
+          if (r == warp)
+            st = xnr[r] - xr[r];
+        const double yt = gn[t] - g[t], gt = gx[t];
+        v[0] = st * yt;
+        v[1] = yt * uu;
+        v[2] = uu * gt;
+        v[3] = st * gt;
+        v[4] = gt * hh;
+        v[5] = gt * gt;
       }
+      v[6] = (double)stop_now;
+      grp.template sum<7>(v); // its barrier publishes u and h
+      const bool skipped = fabs(v[0]) < kMinCurvature;
+      const double sg = v[3], gh = v[4];
+      double rho = 0.0, hb = 0.0, wg = 0.0;
       if (!skipped) {
-        const double yu = grp.sum(yu_part);
-        const double rho = 1.0 / sy;
-        const double hb = 0.5 * rho * fma(rho, yu, 1.0);
-        double wg = 0.0, sg2 = 0.0;
-        for (int i = t; i < D; i += kBlock) {
-          const double wi = fma(hb, s[i], -rho * u[i]);
-          w[i] = wi;
-          wg = fma(wi, gnext[i], wg);
-          sg2 = fma(s[i], gnext[i], sg2);
-        }
-        double v[2] = {wg, sg2};
-        grp.template sum<2>(v); // barriers publish w
-        // sweep 2: H += s w^T + w s^T
-        for (int e = t; e < D * D; e += kBlock) {
-          const int i = e / D, j = e - (e / D) * D;
-          H[e] += __dadd_rn(__dmul_rn(s[i], w[j]), __dmul_rn(w[i], s[j]));
-        }
-        for (int i = t; i < D; i += kBlock)
-          p[i] = -(h[i] + s[i] * v[0] + w[i] * v[1]);
-      } else {
-        for (int i = t; i < D; i += kBlock)
-          p[i] = -h[i];
+        rho = 1.0 / v[0];
+        hb = 0.5 * rho * fma(rho, v[1], 1.0);
+        wg = hb * sg - rho * v[2];
       }
+#pragma unroll
+      for (int r = 0; r < RV; ++r) {
+        const int i = lane + 32 * r;
+        if (i < D) {
+          const double si = xnr[r] - xr[r];
+          if (!skipped) {
+            const double wi = fma(hb, si, -rho * u[i]);
+            pr[r] = -(h[i] + si * wg + wi * sg);
+            if (warp == 0)
+              *reinterpret_cast<double2*>(SW + 2 * i) = make_double2(si, wi);
+          } else {
+            pr[r] = -h[i];
+          }
+        }
+        if (take)
+          xr[r] = xnr[r];
+      }
+      pend = !skipped;
+      ddir = skipped ? -gh : -(gh + 2.0 * sg * wg);
+      stop = v[6] != 0.0;
       if (take) {
         best = fnew;
-        for (int i = t; i < D; i += kBlock) {
-          x[i] = xn[i];
-          g[i] = gn[i];
-        }
+        cur ^= 1;
       }
-      // one reduction: ||g||, the next g.p and the stop flag for the next
-      // iteration's check
-      double v3[3] = {0.0, 0.0, t == 0 ? (double)load_stop(ctl) : 0.0};
-      for (int i = t; i < D; i += kBlock) {
-        v3[0] = fma(g[i], g[i], v3[0]);
-        v3[1] = fma(g[i], p[i], v3[1]);
-      }
-      grp.template sum<3>(v3);
-      const double gnrm = sqrt(v3[0]);
-      ddir = v3[1];
-      stop = v3[2] != 0.0;
+      const double gnrm = sqrt(v[5]);
       if (!isfinite(gnrm) || !isfinite(fnew)) {
         status = kNonFinite;
         fout = fnew;
@@ -604,13 +878,19 @@ namespace zb {
         status = kSurrender;
       fout = best;
       double gg = 0.0;
-      for (int i = t; i < D; i += kBlock)
+      const double* g = gb + cur * D;
+      for (int i = lane; i < D; i += 32)
         gg = fma(g[i], g[i], gg);
-      gout = sqrt(grp.sum(gg));
+      gout = sqrt(warp_allsum(gg));
     }
-    if (out.x)
-      for (int i = t; i < D; i += kBlock)
-        out.x[run * D + i] = x[i];
+    if (warp == 0 && out.x) {
+#pragma unroll
+      for (int r = 0; r < RV; ++r) {
+        const int i = lane + 32 * r;
+        if (i < D)
+          out.x[run * D + i] = xr[r];
+      }
+    }
     if (t == 0) {
       if (out.fval)
         out.fval[run] = fout;
@@ -634,7 +914,7 @@ namespace zb {
     bfgs_cta_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
                     RunOut out, Control* ctl)
   {
-    extern __shared__ double sm[];
+    extern __shared__ __align__(16) double sm[];
     for (int64_t run = blockIdx.x; run < prm.n; run += gridDim.x)
       cta_run<F, D, Adjoint, kBlock>(f, sm, prm, starts + run * D, run, out,
                                      ctl);

@@ -63,7 +63,7 @@ namespace zb {
     bfgs_exact_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
                       RunOut out, Control* ctl, double* __restrict__ scratch)
   {
-    extern __shared__ double sm[];
+    extern __shared__ __align__(16) double sm[];
     double* x = sm;
     double* xn = x + D;
     double* g = xn + D;

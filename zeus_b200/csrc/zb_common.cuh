@@ -26,6 +26,19 @@ namespace zb {
   inline constexpr int kLineSearchTrials = 20;
   inline constexpr double kMinCurvature = 1e-14;
 
+  // 2^-k for 0 <= k <= 1022, built from its exponent bits (the line-search
+  // step sizes alpha_k, exact).
+  __host__ __device__ __forceinline__ double
+  pow2neg(int k)
+  {
+    union {
+      unsigned long long u;
+      double d;
+    } b;
+    b.u = (unsigned long long)(1023 - k) << 52;
+    return b.d;
+  }
+
   struct BfgsParams {
     int64_t n;
     int max_iter;

@@ -72,7 +72,7 @@ namespace zb {
   size_t
   pso_workspace_bytes(int64_t n, int dim)
   {
-    const int64_t blocks = (n + kPsoBlock - 1) / kPsoBlock;
+    const int64_t blocks = pso_blocks(n, dim);
     size_t b = 0;
     b += align_up(sizeof(double) * (size_t)n * dim); // X
     b += align_up(sizeof(double) * (size_t)n * dim); // V
@@ -95,7 +95,7 @@ namespace zb {
       set_error("PSO needs %zu workspace bytes, got %zu", need, ws_bytes);
       return ZEUS_E_WORKSPACE;
     }
-    const int64_t blocks = (n + kPsoBlock - 1) / kPsoBlock;
+    const int64_t blocks = pso_blocks(n, o.dim);
     char* p = static_cast<char*>(ws);
     PsoWork wk;
     wk.X = reinterpret_cast<double*>(p);
@@ -112,11 +112,19 @@ namespace zb {
       using F = decltype(f);
       constexpr int D = (int)F::arity;
       pso_reset_kernel<D><<<1, 256, 0, st>>>(wk);
-      pso_init_kernel<F, D><<<(unsigned)blocks, kPsoBlock, 0, st>>>(
-        f, n, lower, upper, seed, wk, pbx, pbf);
-      for (int t = 1; t <= iters; ++t)
-        pso_iter_kernel<F, D><<<(unsigned)blocks, kPsoBlock, 0, st>>>(
-          f, n, w, c1, c2, seed, t, wk, pbx, pbf);
+      if constexpr (D >= kPsoCoopMinDim) {
+        pso_init_coop_kernel<F, D><<<(unsigned)blocks, kPsoBlock, 0, st>>>(
+          f, n, lower, upper, seed, wk, pbx, pbf);
+        for (int t = 1; t <= iters; ++t)
+          pso_iter_coop_kernel<F, D><<<(unsigned)blocks, kPsoBlock, 0, st>>>(
+            f, n, w, c1, c2, seed, t, wk, pbx, pbf);
+      } else {
+        pso_init_kernel<F, D><<<(unsigned)blocks, kPsoBlock, 0, st>>>(
+          f, n, lower, upper, seed, wk, pbx, pbf);
+        for (int t = 1; t <= iters; ++t)
+          pso_iter_kernel<F, D><<<(unsigned)blocks, kPsoBlock, 0, st>>>(
+            f, n, w, c1, c2, seed, t, wk, pbx, pbf);
+      }
       return cuda_fail(cudaGetLastError(), "PSO launch");
     });
   }

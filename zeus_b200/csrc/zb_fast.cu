@@ -4,26 +4,25 @@
 
 namespace zb {
 
+  // The layout by dimension when neither the configuration nor the
+  // autotuner names one: a thread per run with H in registers for D <= 8, a
+  // warp per run (H rows in lane registers) up to D = 32, a block per run
+  // with H in shared memory above.
   void
   default_layout(int kind, int dim, int* layout, int* tile)
   {
     *tile = 0;
-    if (dim <= 4 && thread_layout_supported(kind, dim)) {
+    if (dim <= 8 && thread_layout_supported(kind, dim)) {
       *layout = ZEUS_LAYOUT_THREAD;
       return;
     }
     const unsigned w = tile_widths(kind, dim);
     if (w) {
-      // narrowest tile whose rows of H fit in about 40 doubles per lane
-      for (int k = 1; k <= 5; ++k) {
-        const int ts = 1 << k;
-        const int r = (dim + ts - 1) / ts;
+      for (int k = 5; k >= 1; --k) // the widest built, a warp when it is
         if ((w >> k) & 1u) {
-          *tile = ts;
-          if (r * dim <= 40)
-            break;
+          *tile = 1 << k;
+          break;
         }
-      }
       *layout = ZEUS_LAYOUT_TILE;
       return;
     }

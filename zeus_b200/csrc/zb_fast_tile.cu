@@ -6,7 +6,8 @@ namespace zb {
 
   namespace {
     // widths built for an objective and dimension: H rows per lane R*D <=
-    // 64 doubles; wider than 2*D only where the cooperative evaluation
+    // 64 doubles; up to 4*D lanes (the spare lanes evaluate line-search
+    // trials in parallel), any width where the cooperative evaluation
     // splits something other than the coordinates (the NLL's bins, the
     // Gaussian's C x)
     constexpr unsigned
@@ -19,7 +20,7 @@ namespace zb {
       for (int k = 1; k <= 5; ++k) {
         const int ts = 1 << k;
         const int r = (d + ts - 1) / ts;
-        if (r * d <= 64 && (wide || ts <= 2 * d))
+        if (r * d <= 64 && (wide || ts <= 4 * d))
           m |= 1u << k;
       }
       return m;

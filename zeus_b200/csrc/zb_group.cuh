@@ -5,7 +5,8 @@
 // Both give the same interface (rank, size, sync, sum, bcast) so objective
 // code is written once for either.  sum() returns identical bits in every
 // member: butterfly partners add the same two values (addition commutes),
-// and the block version has every thread add the per-warp sums in one order.
+// and a value summed by one lane reaches the others by shuffles or shared
+// memory, never re-added.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -13,6 +14,68 @@
 namespace zb {
 
   namespace cg = cooperative_groups;
+
+  // Reduce-scatter of K values over the NL lanes of a warp or tile (NL a
+  // power of two >= P, P = K rounded up to a power of two): at each of the
+  // first log2 P xor levels a lane keeps half of its values and adds the
+  // partner's copy of that half, so the level moves half as many values as
+  // a plain butterfly of all K; the remaining levels add one value.  On
+  // return lane l holds in v[0] the sum of value rs_index(l) over all NL
+  // lanes.  `shx(x, m)` is the xor shuffle of the group.
+  template <int K>
+  struct ReduceScatter {
+    static constexpr int P = K <= 1 ? 1 : K <= 2 ? 2 : K <= 4 ? 4 : 8;
+    static_assert(K <= 8, "at most 8 values");
+
+    template <int NL>
+    __device__ static __forceinline__ int
+    index(int lane)
+    {
+      int idx = 0;
+#pragma unroll
+      for (int h = P / 2, m = NL / 2; h > 0; h >>= 1, m >>= 1)
+        if (lane & m)
+          idx += h;
+      return idx;
+    }
+    // the lowest lane holding value k
+    template <int NL>
+    __device__ static __forceinline__ int
+    owner(int k)
+    {
+      int lane = 0;
+#pragma unroll
+      for (int h = P / 2, m = NL / 2; h > 0; h >>= 1, m >>= 1)
+        if (k & h)
+          lane += m;
+      return lane;
+    }
+    template <int NL, class Shx>
+    __device__ static __forceinline__ double
+    run(const double (&in)[K], int lane, Shx shx)
+    {
+      static_assert(NL >= P, "group narrower than the value count");
+      double v[P];
+#pragma unroll
+      for (int k = 0; k < P; ++k)
+        v[k] = k < K ? in[k] : 0.0;
+      int m = NL / 2;
+#pragma unroll
+      for (int h = P / 2; h > 0; h >>= 1, m >>= 1) {
+        const bool up = (lane & m) != 0;
+#pragma unroll
+        for (int j = 0; j < h; ++j) {
+          const double send = up ? v[j] : v[j + h];
+          const double keep = up ? v[j + h] : v[j];
+          v[j] = keep + shx(send, m);
+        }
+      }
+#pragma unroll
+      for (; m > 0; m >>= 1)
+        v[0] += shx(v[0], m);
+      return v[0];
+    }
+  };
 
   // Every group also carries `scratch`: shared memory of at least size()
   // doubles that objectives may use between two sync()s.
@@ -51,11 +114,22 @@ namespace zb {
     __device__ __forceinline__ void
     sum(double (&v)[K]) const
     {
-#pragma unroll
-      for (int m = TS / 2; m > 0; m >>= 1)
+      using RS = ReduceScatter<K>;
+      if constexpr (K >= 3 && TS >= RS::P) {
+        // reduce-scatter, then every lane fetches each total from its owner
+        const int lane = (int)t.thread_rank();
+        const double mine = RS::template run<TS>(
+          v, lane, [&](double x, int m) { return t.shfl_xor(x, m); });
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          v[k] += t.shfl_xor(v[k], m);
+          v[k] = t.shfl(mine, RS::template owner<TS>(k));
+      } else {
+#pragma unroll
+        for (int m = TS / 2; m > 0; m >>= 1)
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+            v[k] += t.shfl_xor(v[k], m);
+      }
     }
     template <class T>
     __device__ __forceinline__ T
@@ -66,12 +140,16 @@ namespace zb {
   };
 
   // `red` points at kCtaRedDoubles doubles of shared memory reserved for the
-  // group's reductions: two buffers of 32 warps x 8 values used in turn --
-  // every thread runs the same sequence of sums, so a buffer is rewritten
-  // only two sums later, after the barrier of the sum in between, when every
-  // thread has finished reading it: one barrier per sum -- plus one slot for
-  // bcast().  The block size must be a multiple of 32.
-  inline constexpr int kCtaRedDoubles = 2 * 32 * 8 + 8;
+  // group's reductions: two buffers of 8 values x 32 warps used in turn
+  // (every thread runs the same sequence of sums, so a buffer is rewritten
+  // only two sums later, after the barriers of the sum in between, when
+  // every thread has finished with it), 8 totals and one slot for bcast().
+  // A sum: each warp reduce-scatters its values and writes its partials;
+  // barrier; warp 0 reduce-scatters the per-warp partials and writes the
+  // totals; barrier; every thread reads the totals.  (Redundant per-warp
+  // second stages cost more in shuffle throughput than the second barrier.)
+  // The block size must be a multiple of 32.
+  inline constexpr int kCtaRedDoubles = 2 * 32 * 8 + 8 + 8;
 
   struct CtaGroup {
     double* red;
@@ -97,28 +175,34 @@ namespace zb {
     __device__ __forceinline__ void
     sum(double (&v)[K]) const
     {
-      static_assert(K <= 8, "at most 8 simultaneous sums");
-#pragma unroll
-      for (int m = 16; m > 0; m >>= 1)
-#pragma unroll
-        for (int k = 0; k < K; ++k)
-          v[k] += __shfl_xor_sync(0xffffffffu, v[k], m);
+      using RS = ReduceScatter<K>;
+      const auto shx = [](double x, int m) {
+        return __shfl_xor_sync(0xffffffffu, x, m);
+      };
       const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
       const int nw = (blockDim.x + 31) >> 5;
       double* buf = red + parity * (32 * 8);
+      double* tot = red + 2 * 32 * 8;
       parity ^= 1;
-      if (lane == 0)
+      const int idx = RS::template index<32>(lane);
+      const bool owner = (lane & (32 / RS::P - 1)) == 0 && idx < K;
+      const double mine = RS::template run<32>(v, lane, shx);
+      if (owner)
+        buf[idx * 32 + warp] = mine;
+      __syncthreads();
+      if (warp == 0) {
+        double w[K];
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          buf[warp * 8 + k] = v[k];
+          w[k] = lane < nw ? buf[k * 32 + lane] : 0.0;
+        const double t = RS::template run<32>(w, lane, shx);
+        if (owner)
+          tot[idx] = t;
+      }
       __syncthreads();
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        double a = 0.0;
-        for (int w = 0; w < nw; ++w)
-          a += buf[w * 8 + k];
-        v[k] = a;
-      }
+      for (int k = 0; k < K; ++k)
+        v[k] = tot[k];
     }
     __device__ __forceinline__ double
     sum(double v) const
@@ -130,7 +214,7 @@ namespace zb {
     __device__ __forceinline__ double
     bcast(double v, int src) const
     {
-      double* slot = red + 2 * 32 * 8;
+      double* slot = red + 2 * 32 * 8 + 8;
       if ((int)threadIdx.x == src)
         slot[0] = v;
       __syncthreads();

@@ -68,6 +68,27 @@ namespace zeus {
       return sum;
     }
 
+    // f(x + a p) by one thread from interleaved {x_i, p_i} (16-byte loads);
+    // coordinate i of the trial point is fma(a, p_i, x_i), the same bits as
+    // a materialised trial point
+    // (four partial sums: the chain of dependent FMAs is a quarter as long)
+    __device__ double
+    value_line(const double2* xp, double a) const
+    {
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+      double xi = fma(a, xp[0].y, xp[0].x);
+#pragma unroll 8
+      for (std::size_t i = 0; i + 1 < D; ++i) {
+        const double2 q = xp[i + 1];
+        const double xj = fma(a, q.y, q.x);
+        const double t1 = 1.0 - xi;
+        const double t2 = fma(-xi, xi, xj);
+        acc[i & 3] = fma(100.0 * t2, t2, fma(t1, t1, acc[i & 3]));
+        xi = xj;
+      }
+      return (acc[0] + acc[1]) + (acc[2] + acc[3]);
+    }
+
     // d/dx_i: -2(1-x_i) - 400 x_i (x_{i+1}-x_i^2) + 200 (x_i - x_{i-1}^2)
     __host__ __device__ double
     adjoint(const double* x, double* g) const
@@ -117,6 +138,23 @@ namespace zeus {
       }
       return grp.sum(part);
     }
+    // the gradient alone (no reduction): each member writes its coordinates
+    template <class G>
+    __device__ void
+    gradient_coop(const G& grp, const double* x, double* g) const
+    {
+      for (int i = grp.rank(); i < (int)D; i += grp.size()) {
+        double gi = 0.0;
+        if (i + 1 < (int)D) {
+          const double t1 = 1.0 - x[i];
+          const double t2 = fma(-x[i], x[i], x[i + 1]);
+          gi = -2.0 * t1 - 400.0 * x[i] * t2;
+        }
+        if (i > 0)
+          gi = fma(200.0, fma(-x[i - 1], x[i - 1], x[i]), gi);
+        g[i] = gi;
+      }
+    }
   };
 
   template <std::size_t D>
@@ -140,6 +178,19 @@ namespace zeus {
                        T(10.0, 0.0) * dual::cos(x[i] * T(kTwoPi, 0.0)));
         return sum;
       }
+    }
+
+    __device__ double
+    value_line(const double2* xp, double a) const
+    {
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+      for (std::size_t i = 0; i < D; ++i) {
+        const double2 q = xp[i];
+        const double xi = fma(a, q.y, q.x);
+        acc[i & 3] += fma(xi, xi, -10.0 * ::cospi(2.0 * xi));
+      }
+      return 10.0 * D + ((acc[0] + acc[1]) + (acc[2] + acc[3]));
     }
 
     __host__ __device__ double
@@ -187,6 +238,16 @@ namespace zeus {
       }
       return 10.0 * D + grp.sum(part);
     }
+    template <class G>
+    __device__ void
+    gradient_coop(const G& grp, const double* x, double* g) const
+    {
+      for (int i = grp.rank(); i < (int)D; i += grp.size()) {
+        double s, c;
+        ::sincospi(2.0 * x[i], &s, &c);
+        g[i] = fma(10.0 * kTwoPi, s, 2.0 * x[i]);
+      }
+    }
   };
 
   template <std::size_t D>
@@ -218,6 +279,23 @@ namespace zeus {
         const T term2 = T(0.0) - dual::exp(sum_cos / T(double(D)));
         return term1 + term2 + T(20.0) + dual::exp(T(1.0));
       }
+    }
+
+    __device__ double
+    value_line(const double2* xp, double a) const
+    {
+      double s2[2] = {0.0, 0.0}, c2[2] = {0.0, 0.0};
+#pragma unroll 8
+      for (std::size_t i = 0; i < D; ++i) {
+        const double2 q = xp[i];
+        const double xi = fma(a, q.y, q.x);
+        s2[i & 1] = fma(xi, xi, s2[i & 1]);
+        c2[i & 1] += ::cospi(2.0 * xi);
+      }
+      const double ss = s2[0] + s2[1], sc = c2[0] + c2[1];
+      constexpr double inv = 1.0 / double(D);
+      return -20.0 * ::exp(-0.2 * ::sqrt(ss * inv)) - ::exp(sc * inv) + 20.0 +
+             2.718281828459045;
     }
 
     __host__ __device__ double

@@ -15,8 +15,15 @@
 //    can be captured into one CUDA graph.
 // Coefficients w, c1, c2 and the update v <- w v + c1 r1 (pb - x) +
 // c2 r2 (gb - x), x <- x + v are the reference's (pso.cuh:104-119, 302).
+//
+// For D >= kPsoCoopMinDim a warp moves one particle (lane l takes
+// coordinates l, l+32, ...) and evaluates f cooperatively: one thread per
+// particle would serialise O(D^2) work per particle (the 150-D Gaussian)
+// over a handful of SMs.  Positions and velocities are the same bits either
+// way; f differs from the one-thread sum at rounding level.
 #pragma once
 
+#include "zb_bfgs_coop.cuh"
 #include "zb_common.cuh"
 #include "zb_philox.cuh"
 
@@ -32,6 +39,15 @@ namespace zb {
   };
 
   inline constexpr int kPsoBlock = 256;
+  inline constexpr int kPsoCoopMinDim = 33;
+
+  // Blocks of one PSO launch (one per-block minimum slot each).
+  __host__ __device__ inline int64_t
+  pso_blocks(int64_t n, int dim)
+  {
+    const int per = dim >= kPsoCoopMinDim ? kPsoBlock / 32 : kPsoBlock;
+    return (n + per - 1) / per;
+  }
 
   // Block-wide lexicographic min of (key, idx); result valid in thread 0.
   __device__ __forceinline__ void
@@ -188,6 +204,86 @@ namespace zb {
       }
       key = order_key(fv);
       kidx = (int)i;
+    }
+    pso_publish<D>(w, w.X, key, kidx);
+  }
+
+  // Warp-per-particle forms (D >= kPsoCoopMinDim): particle i is warp i of
+  // the grid; the same random counters and update expressions as above.
+  template <class F, int D>
+  __global__ void __launch_bounds__(kPsoBlock)
+    pso_init_coop_kernel(F f, int64_t n, double lower, double upper,
+                         uint64_t seed, PsoWork w, double* __restrict__ pbx,
+                         double* __restrict__ pbf)
+  {
+    __shared__ double scr[kPsoBlock];
+    const int lane = threadIdx.x & 31;
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    unsigned long long key = ~0ull;
+    int kidx = 0x7fffffff;
+    if (i < n) { // warp-uniform
+      const double vr = (upper - lower) * 0.1;
+      for (int d = lane; d < D; d += 32) {
+        const double ux = uniform01(seed, kTagPsoX, (uint64_t)i, (uint32_t)d);
+        const double uv = uniform01(seed, kTagPsoV, (uint64_t)i, (uint32_t)d);
+        const double rx = lower + (upper - lower) * ux;
+        const double rv = -vr + (vr - -vr) * uv;
+        w.X[i * D + d] = rx;
+        w.V[i * D + d] = rv;
+        pbx[i * D + d] = rx;
+      }
+      __syncwarp();
+      const TileGroup<32> grp(cg::tiled_partition<32>(cg::this_thread_block()),
+                              scr + (threadIdx.x & ~31));
+      const double fv = coop_value<F, D>(f, grp, w.X + i * D);
+      if (lane == 0) {
+        pbf[i] = fv;
+        key = order_key(fv);
+        kidx = (int)i;
+      }
+    }
+    pso_publish<D>(w, w.X, key, kidx);
+  }
+
+  template <class F, int D>
+  __global__ void __launch_bounds__(kPsoBlock)
+    pso_iter_coop_kernel(F f, int64_t n, double wi, double c1, double c2,
+                         uint64_t seed, int t, PsoWork w,
+                         double* __restrict__ pbx, double* __restrict__ pbf)
+  {
+    __shared__ double scr[kPsoBlock];
+    const int lane = threadIdx.x & 31;
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    unsigned long long key = ~0ull;
+    int kidx = 0x7fffffff;
+    if (i < n) { // warp-uniform
+      const uint32_t tag = kTagPsoIter + (uint32_t)t;
+      for (int d = lane; d < D; d += 32) {
+        const double r1 = uniform01(seed, tag, (uint64_t)i, 2u * d);
+        const double r2 = uniform01(seed, tag, (uint64_t)i, 2u * d + 1u);
+        const double xi = w.X[i * D + d];
+        const double vi = w.V[i * D + d];
+        const double pb = pbx[i * D + d];
+        const double gb = w.gbest[1 + d];
+        const double nv = wi * vi + c1 * r1 * (pb - xi) + c2 * r2 * (gb - xi);
+        w.V[i * D + d] = nv;
+        w.X[i * D + d] = xi + nv;
+      }
+      __syncwarp();
+      const TileGroup<32> grp(cg::tiled_partition<32>(cg::this_thread_block()),
+                              scr + (threadIdx.x & ~31));
+      const double fv = coop_value<F, D>(f, grp, w.X + i * D);
+      const bool better = fv < pbf[i];
+      if (better)
+        for (int d = lane; d < D; d += 32) // coordinates this lane wrote
+          pbx[i * D + d] = w.X[i * D + d];
+      __syncwarp(); // every lane has read pbf[i]
+      if (lane == 0) {
+        if (better)
+          pbf[i] = fv;
+        key = order_key(fv);
+        kidx = (int)i;
+      }
     }
     pso_publish<D>(w, w.X, key, kidx);
   }

@@ -187,9 +187,10 @@ class BatchJob:
 class Batch:
     """A persistent-batch launch with preallocated workspace."""
 
-    def __init__(self, jobs, max_iter: int = 10000, tol: float = 1e-8, flags: int = 0):
+    def __init__(self, jobs, max_iter: int = 10000, tol: float = 1e-8, flags: int = 0,
+                 block: int = 0):
         self.jobs = list(jobs)
-        self.cfg = make_config(max_iter, 1, tol, "fast", "adjoint", flags=flags)
+        self.cfg = make_config(max_iter, 1, tol, "fast", "adjoint", block=block, flags=flags)
         self.arr = (BatchClass * len(self.jobs))(*[j.c() for j in self.jobs])
         self.wsz = lib().zeus_batch_workspace_size(self.arr, len(self.jobs))
         dev = self.jobs[0].starts.device
@@ -205,9 +206,10 @@ class Batch:
 
 
 def batch_device(jobs, max_iter: int = 10000, tol: float = 1e-8, flags: int = 0,
-                 stream=None) -> Batch:
-    """Runs every BatchJob in one persistent kernel launch."""
-    return Batch(jobs, max_iter, tol, flags).launch(stream)
+                 stream=None, block: int = 0) -> Batch:
+    """Runs every BatchJob in one persistent kernel launch (block: 512 or 384
+    threads, 0 = chosen by the library)."""
+    return Batch(jobs, max_iter, tol, flags, block).launch(stream)
 
 
 def autotune(obj, n_sample: int = 2048, max_iter: int = 10000, tol: float = 1e-8,
