@@ -109,6 +109,20 @@ class Job:
         self.lo, self.hi, self.pso_iter = lo, hi, pso_iter
         self.max_iter, self.required, self.tol = max_iter, required, tol
         self.runs_per_instance = runs_per_instance
+        self.n_full = n  # before --scale: the objective's data holds n_full / rpi instances
+
+    def make_objective(self):
+        """The class's objective; a scaled-down class with per-instance data
+        keeps only the instances its runs use."""
+        obj = self.obj_fn()
+        rpi = self.runs_per_instance
+        if rpi and obj.idata is not None and self.n != self.n_full:
+            import zeus_b200 as zb
+
+            nb = len(obj.idata) // (self.n_full // rpi)
+            used = (self.n + rpi - 1) // rpi
+            obj = zb.PoissonNLL(obj.idata[:used * nb], obj.data[:used * nb])
+        return obj
 
 
 def dijet_objective(toys=512, nbins=100, seed=7):
@@ -291,7 +305,7 @@ def run_gpu(args, rank, world, local_rank):
 
     state = []
     for ci, j in enumerate(jobs):
-        obj = j.obj_fn()
+        obj = j.make_objective()
         dp = DeviceProblem(obj, dev)
         d = obj.dim
         starts = torch.empty((j.n, d), dtype=torch.float64, device=dev)
