@@ -193,7 +193,11 @@ namespace zb {
         status = kStopped;
         break;
       }
-      const int stop_now = lane == 0 ? load_stop(ctl) : 0; // consumed below
+      // This iteration's read of the stop flag (consumed at the reduction)
+      // is issued after a sync and before a stretch of arithmetic: every
+      // sync waits for the thread's outstanding loads, so issued before one
+      // it would stall the tile for a global-memory round trip.
+      int stop_now = 0;
       // ---- line search: alpha_k = 2^-k, first k in 0..19 that passes,
       // else alpha = 2^-20 (utils.cuh:376-412)
       int found = -1;
@@ -207,6 +211,8 @@ namespace zb {
             xs[i] = fma(1.0, p[r], x[r]);
         }
         grp.sync();
+        if (lane == 0)
+          stop_now = load_stop(ctl);
         const double f0 = coop_value<F, D>(f, grp, xs);
         if (f0 <= best + kArmijoC1 * ddir && f0 < best) {
           found = 0;
@@ -224,6 +230,8 @@ namespace zb {
               *reinterpret_cast<double2*>(xp + 2 * i) = make_double2(x[r], p[r]);
           }
           grp.sync();
+          if (!kCoopFirst && lane == 0)
+            stop_now = load_stop(ctl);
           for (int base = k0; found < 0; base += TS) {
             const int k = base + lane;
             double fk = 0.0;
@@ -483,15 +491,31 @@ namespace zb {
     return block >= ncol ? block / ncol : 1;
   }
 
-  // Shared-memory layout (doubles): H[D*D, rounded up to even] | {s,w}[D] |
-  // g[2][D] | u[D] | h[D] | partial sums 2*Q*D | trial point D | (group
-  // trials) one trial point per trial group | trial values 2*32 |
-  // reductions | scratch blockDim.
+  // Rows of H per thread in the sweep; with at most 8 (16 doubles) H lives
+  // in the sweep threads' registers instead of shared memory (D = 64 at
+  // 256-512 threads): the sweep then moves no H bytes at all.
+  __host__ __device__ constexpr int
+  cta_rows_per_thread(int d, int block)
+  {
+    const int q = cta_sweep_q(d, block);
+    return (d + q - 1) / q;
+  }
+  __host__ __device__ constexpr bool
+  cta_h_in_registers(int d, int block)
+  {
+    return d % 2 == 0 && cta_rows_per_thread(d, block) <= 8;
+  }
+
+  // Shared-memory layout (doubles): H[D*D, rounded up to even; none when H
+  // is in registers] | {s,w}[D] | g[2][D] | u[D] | h[D] | partial sums
+  // 2*Q*D | trial point D | (group trials) one trial point per trial group |
+  // trial values 2*32 | reductions | scratch blockDim.
   __host__ __device__ constexpr size_t
   cta_smem_base_doubles(int d, int block)
   {
     const int q = cta_sweep_q(d, block);
-    return (((size_t)d * d + 1) & ~(size_t)1) + 6 * (size_t)d +
+    return (cta_h_in_registers(d, block) ? 0 : (((size_t)d * d + 1) & ~(size_t)1)) +
+           6 * (size_t)d +
            2 * (size_t)q * d + (size_t)d + 64 + kCtaRedDoubles + block;
   }
 
@@ -564,8 +588,11 @@ namespace zb {
     static_assert(kBlock % 32 == 0 && NCOL <= kBlock, "block too small for D");
     static_assert(NG <= 32, "one ballot judges a round");
     static_assert(RV <= NW, "one warp per 32 coordinates at least");
+    constexpr bool kHReg = cta_h_in_registers(D, kBlock);
+    constexpr int RQ = cta_rows_per_thread(D, kBlock);
     double* H = sm;
-    double* SW = H + ((D * D + 1) & ~1); // {s_i, w_i} of the deferred update (16 B)
+    // {s_i, w_i} of the deferred update (16 B aligned)
+    double* SW = H + (kHReg ? 0 : ((D * D + 1) & ~1));
     double* gb = SW + 2 * D;    // two gradient slots of D
     double* u = gb + 2 * D;
     double* h = u + D;
@@ -589,8 +616,20 @@ namespace zb {
     }
     for (int i = t; i < D; i += kBlock)
       xt[i] = x0[i];
-    for (int e = t; e < D * D; e += kBlock)
-      H[e] = (e / D == e % D) ? 1.0 : 0.0;
+    // H = I; with kHReg thread (c, q) keeps rows q, q+Q, ... of columns
+    // C*c .. C*c+C-1 in Hr
+    double Hr[kHReg ? RQ : 1][C];
+    {
+      const int c = t % NCOL, q = t / NCOL;
+#pragma unroll
+      for (int r = 0; r < (kHReg ? RQ : 1); ++r)
+#pragma unroll
+        for (int j = 0; j < C; ++j)
+          Hr[r][j] = (q + Q * r == C * c + j) ? 1.0 : 0.0;
+    }
+    if constexpr (!kHReg)
+      for (int e = t; e < D * D; e += kBlock)
+        H[e] = (e / D == e % D) ? 1.0 : 0.0;
     __syncthreads();
     int cur = 0; // current gradient in slot cur, the new one goes to cur ^ 1
     double best;
@@ -627,9 +666,10 @@ namespace zb {
         status = kStopped;
         break;
       }
-      // this iteration's read of the stop flag, issued now and consumed at
-      // the reduction, so its latency hides behind the line search
-      const int stop_now = t == 0 ? load_stop(ctl) : 0;
+      // this iteration's read of the stop flag, consumed at the reduction:
+      // issued after the line search's first sync, before a stretch of
+      // arithmetic (every barrier waits for the thread's outstanding loads)
+      int stop_now = 0;
       // ---- line search: alpha_k = 2^-k, first k in 0..19 that passes,
       // else alpha = 2^-20 (utils.cuh:376-412)
       double fnew = 0.0, alpha = 1.0;
@@ -658,6 +698,8 @@ namespace zb {
             }
           }
           __syncwarp();
+          if (round == 0 && t == 0)
+            stop_now = load_stop(ctl);
           const int k = r0 + warp * TPW + sub;
           double f1 = 0.0;
           if (k <= kLineSearchTrials) // uniform within the group
@@ -698,6 +740,8 @@ namespace zb {
             }
           }
           __syncthreads();
+          if (k == 0 && t == 0)
+            stop_now = load_stop(ctl);
           double f1;
           if constexpr (kTrialGrad)
             f1 = coop_gradient<F, D, Adjoint>(f, grp, xt, gt);
@@ -738,11 +782,33 @@ namespace zb {
             au[j] = 0.0;
             ah[j] = 0.0;
           }
-          if (pend) {
+          if constexpr (kHReg) {
+#pragma unroll
+            for (int r = 0; r < RQ; ++r) {
+              const int m = q + Q * r;
+              if (m < D) {
+                const double go = g[m], gnm = gn[m];
+                const double gm = take ? gnm : go, ym = gnm - go;
+                if (pend) {
+                  const double2 sw = *reinterpret_cast<const double2*>(SW + 2 * m);
+#pragma unroll
+                  for (int j = 0; j < C; ++j)
+                    Hr[r][j] +=
+                      __dadd_rn(__dmul_rn(sw.x, wi[j]), __dmul_rn(sw.y, si[j]));
+                }
+#pragma unroll
+                for (int j = 0; j < C; ++j) {
+                  ah[j] = fma(Hr[r][j], gm, ah[j]);
+                  au[j] = fma(Hr[r][j], ym, au[j]);
+                }
+              }
+            }
+          } else if (pend) {
 #pragma unroll 4
             for (int m = q; m < D; m += Q) {
               const double2 sw = *reinterpret_cast<const double2*>(SW + 2 * m);
-              const double gm = gx[m], ym = gn[m] - g[m];
+              const double go = g[m], gnm = gn[m];
+              const double gm = take ? gnm : go, ym = gnm - go;
               double* row = H + m * D + i0;
               double hv[C];
               if constexpr (C == 2) {
@@ -768,7 +834,8 @@ namespace zb {
           } else {
 #pragma unroll 4
             for (int m = q; m < D; m += Q) {
-              const double gm = gx[m], ym = gn[m] - g[m];
+              const double go = g[m], gnm = gn[m];
+              const double gm = take ? gnm : go, ym = gnm - go;
               const double* row = H + m * D + i0;
               double hv[C];
               if constexpr (C == 2) {

@@ -27,6 +27,30 @@ namespace zeus {
 
   inline constexpr double kTwoPi = 2.0 * 3.14159265358979323846;
 
+  namespace detail {
+    // Member `grp.rank()` of a cooperating group visits i = rank, rank +
+    // size, ... < N.  For a group whose size is a compile-time constant (a
+    // tile) the loop is unrolled, so its loads issue together instead of
+    // one iteration's loads waiting on the previous iteration's arithmetic.
+    template <int N, class G, class Fn>
+    __device__ __forceinline__ void
+    coop_for(const G& grp, Fn&& fn)
+    {
+      if constexpr (requires { std::integral_constant<int, G::size()>{}; }) {
+        constexpr int S = G::size();
+#pragma unroll
+        for (int k = 0; k < (N + S - 1) / S; ++k) {
+          const int i = grp.rank() + k * S;
+          if (i < N)
+            fn(i);
+        }
+      } else {
+        for (int i = grp.rank(); i < N; i += grp.size())
+          fn(i);
+      }
+    }
+  } // namespace detail
+
   template <std::size_t D>
   struct Rosenbrock {
     static constexpr std::size_t arity = D;
@@ -112,11 +136,11 @@ namespace zeus {
     value_coop(const G& grp, const double* x) const
     {
       double part = 0.0;
-      for (int i = grp.rank(); i < (int)D - 1; i += grp.size()) {
+      detail::coop_for<(int)D - 1>(grp, [&](int i) {
         const double t1 = 1.0 - x[i];
         const double t2 = fma(-x[i], x[i], x[i + 1]);
         part = fma(100.0 * t2, t2, fma(t1, t1, part));
-      }
+      });
       return grp.sum(part);
     }
     template <class G>
@@ -124,7 +148,7 @@ namespace zeus {
     adjoint_coop(const G& grp, const double* x, double* g) const
     {
       double part = 0.0;
-      for (int i = grp.rank(); i < (int)D; i += grp.size()) {
+      detail::coop_for<(int)D>(grp, [&](int i) {
         double gi = 0.0;
         if (i + 1 < (int)D) {
           const double t1 = 1.0 - x[i];
@@ -135,7 +159,7 @@ namespace zeus {
         if (i > 0)
           gi = fma(200.0, fma(-x[i - 1], x[i - 1], x[i]), gi);
         g[i] = gi;
-      }
+      });
       return grp.sum(part);
     }
     // the gradient alone (no reduction): each member writes its coordinates
@@ -143,7 +167,7 @@ namespace zeus {
     __device__ void
     gradient_coop(const G& grp, const double* x, double* g) const
     {
-      for (int i = grp.rank(); i < (int)D; i += grp.size()) {
+      detail::coop_for<(int)D>(grp, [&](int i) {
         double gi = 0.0;
         if (i + 1 < (int)D) {
           const double t1 = 1.0 - x[i];
@@ -153,7 +177,7 @@ namespace zeus {
         if (i > 0)
           gi = fma(200.0, fma(-x[i - 1], x[i - 1], x[i]), gi);
         g[i] = gi;
-      }
+      });
     }
   };
 
@@ -221,8 +245,9 @@ namespace zeus {
     value_coop(const G& grp, const double* x) const
     {
       double part = 0.0;
-      for (int i = grp.rank(); i < (int)D; i += grp.size())
+      detail::coop_for<(int)D>(grp, [&](int i) {
         part += fma(x[i], x[i], -10.0 * ::cospi(2.0 * x[i]));
+      });
       return 10.0 * D + grp.sum(part);
     }
     template <class G>
@@ -230,23 +255,23 @@ namespace zeus {
     adjoint_coop(const G& grp, const double* x, double* g) const
     {
       double part = 0.0;
-      for (int i = grp.rank(); i < (int)D; i += grp.size()) {
+      detail::coop_for<(int)D>(grp, [&](int i) {
         double s, c;
         ::sincospi(2.0 * x[i], &s, &c);
         part += fma(x[i], x[i], -10.0 * c);
         g[i] = fma(10.0 * kTwoPi, s, 2.0 * x[i]);
-      }
+      });
       return 10.0 * D + grp.sum(part);
     }
     template <class G>
     __device__ void
     gradient_coop(const G& grp, const double* x, double* g) const
     {
-      for (int i = grp.rank(); i < (int)D; i += grp.size()) {
+      detail::coop_for<(int)D>(grp, [&](int i) {
         double s, c;
         ::sincospi(2.0 * x[i], &s, &c);
         g[i] = fma(10.0 * kTwoPi, s, 2.0 * x[i]);
-      }
+      });
     }
   };
 
@@ -338,10 +363,10 @@ namespace zeus {
     value_coop(const G& grp, const double* x) const
     {
       double v[2] = {0.0, 0.0};
-      for (int i = grp.rank(); i < (int)D; i += grp.size()) {
+      detail::coop_for<(int)D>(grp, [&](int i) {
         v[0] = fma(x[i], x[i], v[0]);
         v[1] += ::cospi(2.0 * x[i]);
-      }
+      });
       grp.template sum<2>(v);
       constexpr double inv = 1.0 / double(D);
       return -20.0 * ::exp(-0.2 * ::sqrt(v[0] * inv)) - ::exp(v[1] * inv) + 20.0 +
@@ -352,20 +377,19 @@ namespace zeus {
     adjoint_coop(const G& grp, const double* x, double* g) const
     {
       double v[2] = {0.0, 0.0};
-      for (int i = grp.rank(); i < (int)D; i += grp.size()) {
+      detail::coop_for<(int)D>(grp, [&](int i) {
         double s, c;
         ::sincospi(2.0 * x[i], &s, &c);
         v[0] = fma(x[i], x[i], v[0]);
         v[1] += c;
         g[i] = s; // the same member finishes g[i] below
-      }
+      });
       grp.template sum<2>(v);
       constexpr double inv = 1.0 / double(D);
       const double r = ::sqrt(v[0] * inv);
       const double e1 = ::exp(-0.2 * r), e2 = ::exp(v[1] * inv);
       const double a = 4.0 * e1 * inv / r, b = kTwoPi * e2 * inv;
-      for (int i = grp.rank(); i < (int)D; i += grp.size())
-        g[i] = fma(a, x[i], b * g[i]);
+      detail::coop_for<(int)D>(grp, [&](int i) { g[i] = fma(a, x[i], b * g[i]); });
       return -20.0 * e1 - e2 + 20.0 + 2.718281828459045;
     }
   };
