@@ -97,6 +97,21 @@ def algorithmic_flops(jobs_counters) -> float:
     return float(total)
 
 
+# ---------------------------------------------------------------- ranks
+def job_totals(units: float, ms: float, world: int, device) -> tuple[float, float]:
+    """Whole-job (units summed over ranks, step time = the slowest rank's).
+    Every rank calls it at the same point (two collectives)."""
+    if world <= 1:
+        return units, ms
+    import torch
+
+    t_units = torch.tensor([units], dtype=torch.float64, device=device)
+    t_ms = torch.tensor([ms], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t_units, op=torch.distributed.ReduceOp.SUM)
+    torch.distributed.all_reduce(t_ms, op=torch.distributed.ReduceOp.MAX)
+    return float(t_units[0]), float(t_ms[0])
+
+
 # ---------------------------------------------------------------- workloads
 class Job:
     """One class of a workload: objective, runs, bounds, PSO iterations (<0:
@@ -444,15 +459,7 @@ def run_gpu(args, rank, world, local_rank):
 
     step_ms = float(np.mean(times))
     conv_mean = float(np.mean(conv))
-    if world > 1:
-        t = torch.tensor([step_ms, conv_mean], dtype=torch.float64, device=dev)
-        mx = t.clone()
-        torch.distributed.all_reduce(mx, op=torch.distributed.ReduceOp.MAX)
-        sm = t.clone()
-        torch.distributed.all_reduce(sm, op=torch.distributed.ReduceOp.SUM)
-        step_ms_all, conv_all = float(mx[0]), float(sm[1])
-    else:
-        step_ms_all, conv_all = step_ms, conv_mean
+    conv_all, step_ms_all = job_totals(conv_mean, step_ms, world, dev)
     value = conv_all / (step_ms_all * 1e-3)
 
     flops = algorithmic_flops(counters)
@@ -548,11 +555,9 @@ def run_gpu(args, rank, world, local_rank):
         if k >= args.warmup:
             e2e_ms.append((t_b - t_a) * 1e3)
             e2e_conv.append(int(cen_host[:, 1].sum()))
-    e2e_val = float(np.mean(e2e_conv)) / (float(np.mean(e2e_ms)) * 1e-3)
-    if world > 1:
-        t = torch.tensor([e2e_val], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.SUM)
-        e2e_val = float(t[0])
+    e2e_units, e2e_ms_all = job_totals(float(np.mean(e2e_conv)), float(np.mean(e2e_ms)),
+                                       world, dev)
+    e2e_val = e2e_units / (e2e_ms_all * 1e-3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -588,7 +593,7 @@ def run_gpu(args, rank, world, local_rank):
                                         "(zeus_probe_fp64)",
                          "flops_per_step": flops, "kernel_ms": kms, "traffic": None},
             "e2e": {"value": e2e_val, "unit": "runs/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": float(np.mean(e2e_ms))},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms_all},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,

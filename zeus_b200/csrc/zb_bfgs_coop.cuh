@@ -17,9 +17,10 @@
 //
 // Both keep the reference's iteration semantics (line search, skip rule,
 // accept-if-better, status protocol) and the fixed-point exit.  The update
-// H+ = H + s w^T + w s^T forms each product with __dmul_rn so that entry
-// (i, j) and (j, i) round identically and H stays exactly symmetric (the
-// CTA kernel reads columns as rows).
+// H+ = H + s w^T + w s^T: the CTA kernel forms each product with __dmul_rn
+// so that entry (i, j) and (j, i) round identically and H stays exactly
+// symmetric (it reads columns as rows); the tile kernel reads its rows as
+// rows and applies the update as two FMAs.
 #pragma once
 
 #include "zb_bfgs_thread.cuh"
@@ -313,7 +314,8 @@ namespace zb {
             const double2 yg = *reinterpret_cast<const double2*>(quad + 4 * j + 2);
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-              H[r][j] += __dadd_rn(__dmul_rn(sp[r], sw.y), __dmul_rn(wp[r], sw.x));
+              // rows are read as rows here: two FMAs, no symmetric rounding
+              H[r][j] = fma(sp[r], sw.y, fma(wp[r], sw.x, H[r][j]));
               ua[r][j & 1] = fma(H[r][j], yg.x, ua[r][j & 1]);
               ha[r][j & 1] = fma(H[r][j], yg.y, ha[r][j & 1]);
             }
@@ -500,22 +502,32 @@ namespace zb {
     const int q = cta_sweep_q(d, block);
     return (d + q - 1) / q;
   }
+  // D <= 64, D % 8 == 0: column-warps. Warp w < D/8 owns columns
+  // 8w .. 8w+7; its four lane quarters take rows q, q+4, ... (D/4 doubles
+  // of H per lane), and a column's four partial sums meet by two shuffles:
+  // no partial sums in shared memory and no barrier after the sweep.
+  __host__ __device__ constexpr bool
+  cta_col_warps(int d, int block)
+  {
+    return d % 8 == 0 && d <= 64 && d / 8 <= block / 32;
+  }
   __host__ __device__ constexpr bool
   cta_h_in_registers(int d, int block)
   {
-    return d % 2 == 0 && cta_rows_per_thread(d, block) <= 8;
+    return cta_col_warps(d, block) ||
+           (d % 2 == 0 && cta_rows_per_thread(d, block) <= 8);
   }
 
   // Shared-memory layout (doubles): H[D*D, rounded up to even; none when H
-  // is in registers] | {s,w}[D] | g[2][D] | u[D] | h[D] | partial sums
-  // 2*Q*D | trial point D | (group trials) one trial point per trial group |
-  // trial values 2*32 | reductions | scratch blockDim.
+  // is in registers] | {s,w}[D] | g[2][D] | u[D] | h[D] | x[D] | partial
+  // sums 2*Q*D | trial point D | (group trials) one trial point per trial
+  // group | trial values 2*32 | reductions | scratch blockDim.
   __host__ __device__ constexpr size_t
   cta_smem_base_doubles(int d, int block)
   {
     const int q = cta_sweep_q(d, block);
     return (cta_h_in_registers(d, block) ? 0 : (((size_t)d * d + 1) & ~(size_t)1)) +
-           6 * (size_t)d +
+           7 * (size_t)d +
            2 * (size_t)q * d + (size_t)d + 64 + kCtaRedDoubles + block;
   }
 
@@ -588,15 +600,17 @@ namespace zb {
     static_assert(kBlock % 32 == 0 && NCOL <= kBlock, "block too small for D");
     static_assert(NG <= 32, "one ballot judges a round");
     static_assert(RV <= NW, "one warp per 32 coordinates at least");
-    constexpr bool kHReg = cta_h_in_registers(D, kBlock);
+    constexpr bool kColWarp = cta_col_warps(D, kBlock);
+    constexpr bool kHReg = cta_h_in_registers(D, kBlock) && !kColWarp;
     constexpr int RQ = cta_rows_per_thread(D, kBlock);
     double* H = sm;
     // {s_i, w_i} of the deferred update (16 B aligned)
-    double* SW = H + (kHReg ? 0 : ((D * D + 1) & ~1));
+    double* SW = H + (kHReg || kColWarp ? 0 : ((D * D + 1) & ~1));
     double* gb = SW + 2 * D;    // two gradient slots of D
     double* u = gb + 2 * D;
     double* h = u + D;
-    double* partU = h + D;
+    double* xcur = h + D; // x, for the column-warp sweep
+    double* partU = xcur + D;
     double* partH = partU + Q * D;
     double* xt = partH + Q * D; // block trial point / start
     double* trial_x = xt + D;   // NG x D when kWarpTrials
@@ -627,9 +641,17 @@ namespace zb {
         for (int j = 0; j < C; ++j)
           Hr[r][j] = (q + Q * r == C * c + j) ? 1.0 : 0.0;
     }
-    if constexpr (!kHReg)
+    // with kColWarp lane (w, l) keeps rows q, q+4, ... (q = l / 8) of
+    // column 8w + l % 8 in Hc
+    double Hc[kColWarp ? D / 4 : 1];
+#pragma unroll
+    for (int k = 0; k < (kColWarp ? D / 4 : 1); ++k)
+      Hc[k] = (4 * k + (lane >> 3) == warp * 8 + (lane & 7)) ? 1.0 : 0.0;
+    if constexpr (!kHReg && !kColWarp)
       for (int e = t; e < D * D; e += kBlock)
         H[e] = (e / D == e % D) ? 1.0 : 0.0;
+    for (int i = t; i < D; i += kBlock)
+      xcur[i] = x0[i];
     __syncthreads();
     int cur = 0; // current gradient in slot cur, the new one goes to cur ^ 1
     double best;
@@ -769,8 +791,45 @@ namespace zb {
       const bool take = fnew < best;
       const double* gx = take ? gn : g; // the gradient p+ is formed for
 
-      // ---- sweep: deferred update + column partial sums of H y and H g_next
-      {
+      // ---- sweep: deferred update + column sums of H y and H g_next, and
+      // the seven values of the iteration's one reduction
+      double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      if constexpr (kColWarp) {
+        if (warp < D / 8) {
+          const int i = warp * 8 + (lane & 7), q = lane >> 3;
+          const double si = pend ? SW[2 * i] : 0.0, wi = pend ? SW[2 * i + 1] : 0.0;
+          double au2[2] = {0.0, 0.0}, ah2[2] = {0.0, 0.0};
+#pragma unroll
+          for (int k = 0; k < D / 4; ++k) {
+            const int m = 4 * k + q;
+            const double go = g[m], gnm = gn[m];
+            const double gm = take ? gnm : go, ym = gnm - go;
+            if (pend) {
+              const double2 sw = *reinterpret_cast<const double2*>(SW + 2 * m);
+              Hc[k] += __dadd_rn(__dmul_rn(sw.x, wi), __dmul_rn(sw.y, si));
+            }
+            ah2[k & 1] = fma(Hc[k], gm, ah2[k & 1]);
+            au2[k & 1] = fma(Hc[k], ym, au2[k & 1]);
+          }
+          double uu = au2[0] + au2[1], hh = ah2[0] + ah2[1];
+          uu += __shfl_xor_sync(0xffffffffu, uu, 8);
+          hh += __shfl_xor_sync(0xffffffffu, hh, 8);
+          uu += __shfl_xor_sync(0xffffffffu, uu, 16);
+          hh += __shfl_xor_sync(0xffffffffu, hh, 16);
+          if (q == 0) {
+            u[i] = uu;
+            h[i] = hh;
+            const double st = xn_s[i] - xcur[i]; // the registers' s_i, bit for bit
+            const double yt = gn[i] - g[i], gt = gx[i];
+            v[0] = st * yt;
+            v[1] = yt * uu;
+            v[2] = uu * gt;
+            v[3] = st * gt;
+            v[4] = gt * hh;
+            v[5] = gt * gt;
+          }
+        }
+      } else {
         const int c = t % NCOL, q = t / NCOL;
         if (q < Q) {
           const int i0 = C * c;
@@ -858,11 +917,9 @@ namespace zb {
             partH[q * D + i0 + j] = ah[j];
           }
         }
-      }
       __syncthreads();
 
-      // ---- one reduction for every scalar of the update and the checks
-      double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      // ---- the seven values from the column partial sums
       if (t < D) { // coordinate t is slot r = warp of this lane
         double uu = 0.0, hh = 0.0;
 #pragma unroll 4
@@ -885,6 +942,7 @@ namespace zb {
         v[4] = gt * hh;
         v[5] = gt * gt;
       }
+      } // column-warp / shared-memory sweep
       v[6] = (double)stop_now;
       grp.template sum<7>(v); // its barrier publishes u and h
       const bool skipped = fabs(v[0]) < kMinCurvature;
@@ -909,8 +967,11 @@ namespace zb {
             pr[r] = -h[i];
           }
         }
-        if (take)
+        if (take) {
           xr[r] = xnr[r];
+          if (kColWarp && warp == 0 && i < D)
+            xcur[i] = xnr[r];
+        }
       }
       pend = !skipped;
       ddir = skipped ? -gh : -(gh + 2.0 * sg * wg);

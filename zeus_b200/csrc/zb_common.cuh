@@ -31,12 +31,16 @@ namespace zb {
   __host__ __device__ __forceinline__ double
   pow2neg(int k)
   {
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double((long long)(1023 - k) << 52);
+#else
     union {
       unsigned long long u;
       double d;
     } b;
     b.u = (unsigned long long)(1023 - k) << 52;
     return b.d;
+#endif
   }
 
   struct BfgsParams {
