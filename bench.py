@@ -97,6 +97,24 @@ def algorithmic_flops(jobs_counters) -> float:
     return float(total)
 
 
+# ---------------------------------------------------------------- traffic
+# DRAM bytes (read + write) of one batch-kernel launch, from an ncu capture
+# of the 1/8-size mixed batch (0.543 MB read, 512 B written; the ncu summary
+# for the batch kernel under profiles/), scaled to the full batch by its
+# runs (the bytes are the starts read and the results written, proportional
+# to the runs).
+MEASURED_TRAFFIC = {"mixed": 8 * (542976 + 512)}
+
+
+def traffic_of(workload: str) -> dict:
+    t = MEASURED_TRAFFIC.get(workload)
+    if t is None:
+        return {"traffic": None}
+    return {"traffic": t, "traffic_unit": "bytes per launch",
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, 1/8-size "
+                              "capture x 8 (batch-kernel ncu summary under profiles/)"}
+
+
 # ---------------------------------------------------------------- ranks
 def job_totals(units: float, ms: float, world: int, device) -> tuple[float, float]:
     """Whole-job (units summed over ranks, step time = the slowest rank's).
@@ -591,7 +609,8 @@ def run_gpu(args, rank, world, local_rank):
                          "frac": (achieved / peak) if peak else None,
                          "peak_source": "measured FP64 FMA probe on this GPU "
                                         "(zeus_probe_fp64)",
-                         "flops_per_step": flops, "kernel_ms": kms, "traffic": None},
+                         "flops_per_step": flops, "kernel_ms": kms,
+                         **traffic_of(args.workload)},
             "e2e": {"value": e2e_val, "unit": "runs/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms_all},
             "gpu_launches": launches,
