@@ -489,6 +489,29 @@ namespace zeus {
       grp.sync();
     }
 
+    // f alone, 0.5 x.(C^T x): member t forms (C^T x)_i for its columns i
+    // (reads of C coalesced across members); used where a whole f is
+    // evaluated by a small group (a PSO particle's warp, line-search trial
+    // groups of the dual-gradient form).
+    template <class G>
+    __device__ double
+    value_coop(const G& grp, const double* x) const
+    {
+      double part = 0.0;
+      detail::coop_for<(int)D>(grp, [&](int i) {
+        double a0 = 0.0, a1 = 0.0;
+        int j = 0;
+        for (; j + 1 < (int)D; j += 2) {
+          a0 = fma(C[j * D + i], x[j], a0);
+          a1 = fma(C[(j + 1) * D + i], x[j + 1], a1);
+        }
+        if (j < (int)D)
+          a0 = fma(C[j * D + i], x[j], a0);
+        part = fma(x[i], a0 + a1, part);
+      });
+      return 0.5 * grp.sum(part);
+    }
+
     // f = 0.5 x.(C^T x); g = C^T x (symmetric C) else (C x + C^T x) / 2.
     // `g` must be shared by the group (it is written by one member per i
     // and read back by all after the final sync).
