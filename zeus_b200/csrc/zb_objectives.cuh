@@ -473,9 +473,20 @@ namespace zeus {
       }
       const int i = t % (int)D, q = t / (int)D;
       double a = 0.0;
-      if (q < nq)
-        for (int j = q; j < (int)D; j += nq)
+      if (q < nq) {
+        // C comes from L2 (it does not fit beside H in shared memory):
+        // unrolled with two sums so that many loads are in flight at once
+        double a1 = 0.0;
+        int j = q;
+#pragma unroll 8
+        for (; j + nq < (int)D; j += 2 * nq) {
           a = fma(M[j * D + i], x[j], a);
+          a1 = fma(M[(j + nq) * D + i], x[j + nq], a1);
+        }
+        if (j < (int)D)
+          a = fma(M[j * D + i], x[j], a);
+        a += a1;
+      }
       grp.sync();
       if (q < nq)
         grp.scratch[q * D + i] = a;
