@@ -41,6 +41,7 @@
 
 #include "zeus_b200.h"
 #include "zb_bfgs_coop.cuh"
+#include "zb_bfgs_exact.cuh"
 #include "zb_bfgs_thread.cuh"
 #include "zb_dual.cuh"
 #include "zb_pso.cuh"
@@ -348,7 +349,13 @@ namespace zeus {
   // prng_type and nzerosteps are accepted for source compatibility: the
   // layout follows the dimension, starts and PSO draws come from Philox, and
   // the zero-step limit cannot trigger (the reference's line search never
-  // returns 0, utils.cuh:395-411).  trajectory_file is not written.
+  // returns 0, utils.cuh:395-411).  With a trajectory_file (.tsv) the BFGS
+  // runs in exact mode, one run per block in the reference's operation
+  // order, recording every iteration (N * MAX_ITER steps, as the reference
+  // allocates them), and the file is written in the reference's layout
+  // (zeus.cuh:62-103, 189-239; src/utils.cu:128-176); a file that cannot be
+  // written is reported on stderr and the result is still returned, as the
+  // reference does.
   template <typename Function, std::size_t ZEUS_DIM = FnTraits<Function>::arity>
     requires ZeusObjective<Function, ZEUS_DIM>
   Result<ZEUS_DIM>
@@ -360,7 +367,6 @@ namespace zeus {
   {
     (void)parallel;
     (void)prng_type;
-    (void)trajectory_file;
     (void)nzerosteps;
     (void)run;
     constexpr std::size_t D = ZEUS_DIM;
@@ -408,12 +414,57 @@ namespace zeus {
       zb::BfgsParams prm{n, MAX_ITER, requiredConverged, tolerance, 0};
       zb::RunOut out{fval,   status,  iter,    gnorm,   x,
                      nullptr, nullptr, nullptr, nullptr, nullptr};
+      const bool traj = !trajectory_file.empty() && MAX_ITER > 0;
+      const size_t steps = traj ? (size_t)N * (size_t)MAX_ITER : 0;
+      if (traj) {
+        out.traj_x = b.alloc<double>(steps * D);
+        out.traj_f = b.alloc<double>(steps);
+        out.traj_g = b.alloc<double>(steps);
+        out.traj_status = b.alloc<int8_t>(steps);
+        // all-ones bytes: NaN doubles and status -1 (the reference's fill)
+        cudaMemsetAsync(out.traj_x, 0xff, steps * D * sizeof(double), b.st);
+        cudaMemsetAsync(out.traj_f, 0xff, steps * sizeof(double), b.st);
+        cudaMemsetAsync(out.traj_g, 0xff, steps * sizeof(double), b.st);
+        cudaMemsetAsync(out.traj_status, 0xff, steps, b.st);
+      }
       cudaEventRecord(e0, b.st);
-      cudaError_t e = detail::launch_bfgs<Function, D>(
-        f, prm, starts, out, reinterpret_cast<zb::Control*>(ctl), b.st);
+      cudaError_t e;
+      if (traj) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int64_t grid = n < (int64_t)sms * 4 ? n : (int64_t)sms * 4;
+        double* scratch = b.alloc<double>((size_t)grid * 2 * D * D);
+        zb::bfgs_exact_kernel<Function, (int)D, true>
+          <<<(unsigned)grid, 128, zb::exact_smem_bytes<(int)D>(), b.st>>>(
+            f, prm, starts, out, reinterpret_cast<zb::Control*>(ctl), scratch);
+        e = cudaGetLastError();
+      } else {
+        e = detail::launch_bfgs<Function, D>(
+          f, prm, starts, out, reinterpret_cast<zb::Control*>(ctl), b.st);
+      }
       cudaEventRecord(e1, b.st);
       if (e != cudaSuccess)
         throw e;
+      if (traj) {
+        std::vector<double> hx(steps * D), hf(steps), hg(steps);
+        std::vector<int8_t> hs(steps);
+        cudaMemcpyAsync(hx.data(), out.traj_x, hx.size() * sizeof(double),
+                        cudaMemcpyDeviceToHost, b.st);
+        cudaMemcpyAsync(hf.data(), out.traj_f, hf.size() * sizeof(double),
+                        cudaMemcpyDeviceToHost, b.st);
+        cudaMemcpyAsync(hg.data(), out.traj_g, hg.size() * sizeof(double),
+                        cudaMemcpyDeviceToHost, b.st);
+        cudaMemcpyAsync(hs.data(), out.traj_status, hs.size(),
+                        cudaMemcpyDeviceToHost, b.st);
+        if ((e = cudaStreamSynchronize(b.st)) != cudaSuccess)
+          throw e;
+        const std::string path(trajectory_file);
+        if (zeus_write_trajectory_tsv(path.c_str(), hx.data(), hf.data(), hg.data(),
+                                      hs.data(), nullptr, n, MAX_ITER,
+                                      (int32_t)D) != ZEUS_OK)
+          std::fprintf(stderr, "Error: %s\n", zeus_last_error());
+      }
       std::vector<double> km;
       if (fun_name == "rosenbrock")
         km.assign(D, 1.0);

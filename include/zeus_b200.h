@@ -301,6 +301,22 @@ int zeus_optimize(const zeus_problem* host_problem, double lower,
                   double* best_x, zeus_census* census, double* per_run_fval,
                   int32_t* per_run_status, void* stream);
 
+/* ---- trajectory files -------------------------------------------------
+ * Replaces util::writeTrajectoryData's TSV form (src/utils.cu:128-176,
+ * 258-286): writes `path` (must end in .tsv) with the header
+ * "traj step fval grad status alpha x0 .. x{dim-1}" (tab-separated) and one
+ * row per run and step, all max_iter steps of every run, values as %.17e
+ * (the reference's scientific, precision 17), NaN printed "NaN".  The
+ * arrays are HOST copies of an exact-mode run's trajectory buffers
+ * (zeus_run_outputs layouts: coords[step][dim][run], fval / gnorm /
+ * status[step][run]); alpha (same layout) may be NULL for zeros, which is
+ * what the reference's sequential path writes.  The reference's .nc form
+ * needs NetCDF and is not built: such paths return ZEUS_E_UNSUPPORTED. */
+int zeus_write_trajectory_tsv(const char* path, const double* coords,
+                              const double* fval, const double* gnorm,
+                              const int8_t* status, const double* alpha,
+                              int64_t n, int32_t max_iter, int32_t dim);
+
 /* ---- measurement ----------------------------------------------------
  * No counterpart in the reference: a roofline probe.  Runs `iters`
  * iterations of 8 independent FP64 FMA chains per thread on a grid sized to

@@ -95,7 +95,7 @@ emit(const char* name, const zeus::Result<D>& r)
 }
 
 int
-main()
+main(int argc, char** argv)
 {
   emit("rosenbrock", zeus::Zeus(MyRosenbrock{}, -5.0, 5.0, 1024, 10000, 10, 100,
                                 "rosenbrock", 1e-8, 42, 0));
@@ -113,5 +113,8 @@ main()
                               1e-8, 9, 0));
   emit("empty", zeus::Zeus(MyRosenbrock{}, -5.0, 5.0, 0, 100, 10, 10, "rosenbrock", 1e-8,
                            42, 0));
+  if (argc > 1) // trajectory file: exact mode, every iteration recorded
+    emit("traj", zeus::Zeus(MyRosenbrock{}, -5.0, 5.0, 6, 40, -1, 1000, "rosenbrock",
+                            1e-8, 42, 0, true, zeus::PRNGType::XORWOW, argv[1]));
   return 0;
 }

@@ -13,14 +13,40 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.fixture(scope="module")
-def results(cuda):
+def traj_path(tmp_path_factory):
+    return tmp_path_factory.mktemp("dropin") / "traj.tsv"
+
+
+@pytest.fixture(scope="module")
+def results(cuda, traj_path):
     exe = zbuild.DROPIN_BIN
     if not exe.exists():
         pytest.fail(f"{exe} is missing: run zeus_b200/build.py (build_dropin_test)")
-    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    out = subprocess.run([str(exe), str(traj_path)], capture_output=True, text=True,
+                         timeout=300)
     assert out.returncode == 0, out.stderr
     return {d["case"]: d for d in (json.loads(l) for l in out.stdout.splitlines()
                                    if l.startswith("{"))}
+
+
+def test_trajectory_file_from_the_drop_in(results, traj_path):
+    """Zeus(..., trajectory_file) writes the reference's TSV: every run's
+    MAX_ITER steps, step 0 at the injected start."""
+    from tests import _oracle as O
+
+    rows = traj_path.read_text().splitlines()
+    assert rows[0].split("\t") == ["traj", "step", "fval", "grad", "status", "alpha",
+                                    "x0", "x1"]
+    assert len(rows) == 1 + 6 * 40
+    st = O.oracle_starts(42, 6, 2, -5.0, 5.0)
+    for i in range(6):
+        r0 = rows[1 + 40 * i].split("\t")
+        assert (int(r0[0]), int(r0[1])) == (i, 0)
+        np.testing.assert_array_equal([float(r0[6]), float(r0[7])], st[i])
+        f0 = (1 - st[i, 0]) ** 2 + 100 * (st[i, 1] - st[i, 0] ** 2) ** 2
+        np.testing.assert_allclose(float(r0[2]), f0, rtol=1e-13)
+    r = results["traj"]
+    assert r["status"] in (0, 1)
 
 
 def test_rosenbrock_functor(results):

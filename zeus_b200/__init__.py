@@ -165,6 +165,8 @@ SIGNATURES = {
                   _P]),
     "zeus_nll_sensitivity_device": (
         C.c_int, [C.POINTER(Problem), C.c_int64, C.c_int64, _P, _P, _P, _P, _P]),
+    "zeus_write_trajectory_tsv": (
+        C.c_int, [C.c_char_p, _P, _P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32]),
     "zeus_autotune": (
         C.c_int,
         [C.POINTER(Problem), C.POINTER(BfgsConfig), C.c_int64, C.c_uint64, C.c_double,
@@ -323,16 +325,19 @@ def Zeus(f: Objective, lower: float, upper: float, N: int, MAX_ITER: int,
          nzerosteps: int = 0, *, mode: str = "fast", gradient: str = "adjoint",
          per_run: bool = False, stream=None) -> Result:
     """The reference's zeus::Zeus on a built-in objective, host buffers in and
-    out.  ``parallel``/``prng``/``trajectory_file``/``nzerosteps`` are accepted
-    for signature compatibility: the layout is chosen by dimension, the
-    generator is Philox, per-iteration trajectories come from exact mode
-    through bfgs_device(), and the zero-step limit cannot trigger because the
-    reference's line search never returns 0 (utils.cuh:395-411)."""
+    out.  ``parallel``/``prng``/``nzerosteps`` are accepted for signature
+    compatibility: the layout is chosen by dimension, the generator is
+    Philox, and the zero-step limit cannot trigger because the reference's
+    line search never returns 0 (utils.cuh:395-411).  A ``trajectory_file``
+    (``.tsv``) runs the BFGS in exact mode, which records every iteration,
+    and writes the reference's trajectory file (zeus.cuh:62-103, 189-239)."""
     del parallel, prng, run, nzerosteps, fun_name
-    if trajectory_file:
-        raise NotImplementedError("trajectory files: use bfgs_device(..., traj=True)")
     if N < 0:
         raise ValueError("N must be >= 0")
+    if trajectory_file:
+        return _zeus_with_trajectories(f, lower, upper, N, MAX_ITER, PSO_ITER,
+                                       requiredConverged, tolerance, seed,
+                                       trajectory_file, per_run, stream)
     cfg = make_config(MAX_ITER, requiredConverged, tolerance, mode, gradient)
     best = CResult()
     census = CCensus()
@@ -358,11 +363,58 @@ def Zeus(f: Objective, lower: float, upper: float, N: int, MAX_ITER: int,
     return r
 
 
+def write_trajectory_tsv(path: str, traj: dict, alpha=None) -> None:
+    """Writes an exact-mode run's trajectory buffers (BfgsRun.traj) in the
+    reference's TSV layout (src/utils.cu:128-176)."""
+    host = {k: np.ascontiguousarray(v.cpu().numpy()) for k, v in traj.items()}
+    T, dim, n = host["x"].shape
+    a = None if alpha is None else np.ascontiguousarray(alpha, dtype=np.float64)
+    check(lib().zeus_write_trajectory_tsv(
+        str(path).encode(), host["x"].ctypes.data, host["f"].ctypes.data,
+        host["g"].ctypes.data, host["status"].ctypes.data,
+        None if a is None else a.ctypes.data, n, T, dim))
+
+
+def _zeus_with_trajectories(f, lower, upper, N, MAX_ITER, PSO_ITER, required, tol, seed,
+                            path, per_run, stream) -> "Result":
+    """Zeus with a trajectory file: PSO (or uniform) starts, exact-mode BFGS
+    recording every iteration, the census, then the file."""
+    import torch
+
+    from .device import bfgs_device, census_device, pso_device, starts_uniform
+
+    if not str(path).endswith(".tsv"):
+        check(lib().zeus_write_trajectory_tsv(str(path).encode(), None, None, None, None,
+                                              None, 0, 0, f.dim))
+    if N == 0:
+        return Result()
+    if PSO_ITER >= 0:
+        starts, _, _ = pso_device(f, seed & 0xFFFFFFFFFFFFFFFF, N, lower, upper, PSO_ITER)
+    else:
+        starts = starts_uniform(seed & 0xFFFFFFFFFFFFFFFF, N, f.dim, lower, upper)
+    r = bfgs_device(f, starts, max_iter=MAX_ITER, required=required, tol=tol,
+                    mode="exact", gradient="dual", traj=True, stream=stream)
+    cen = census_device(r.fval, r.status, r.x, f.dim,
+                        np.ones(f.dim) if f.kind == OBJ_ROSENBROCK else None)
+    torch.cuda.synchronize()
+    write_trajectory_tsv(path, r.traj)
+    idx = int(cen["best_idx"])
+    out = Result(idx=idx, status=int(r.status[idx]), fval=float(r.fval[idx]),
+                 gradientNorm=float(r.gnorm[idx]), coordinates=r.x[idx].cpu().numpy(),
+                 iter=int(r.iter[idx]),
+                 c=Convergence(cen["actual"], cen["claimed"], cen["surrendered"],
+                               cen["stopped"]))
+    if per_run:
+        out.per_run_fval = r.fval.cpu().numpy()
+        out.per_run_status = r.status.cpu().numpy()
+    return out
+
+
 from .device import (bfgs_device, pso_device, starts_uniform, census_device,  # noqa: E402
                      batch_device, autotune, BatchJob)
 
 __all__ = [
-    "Zeus", "Result", "Convergence", "Objective", "Rosenbrock", "Rastrigin",
+    "Zeus", "write_trajectory_tsv", "Result", "Convergence", "Objective", "Rosenbrock", "Rastrigin",
     "Ackley", "Gaussian", "PoissonNLL", "gaussian_matrix", "bfgs_device",
     "pso_device", "starts_uniform", "census_device", "lib", "supported",
     "batch_device", "autotune", "BatchJob",
