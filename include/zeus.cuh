@@ -355,7 +355,9 @@ namespace zeus {
   // allocates them), and the file is written in the reference's layout
   // (zeus.cuh:62-103, 189-239; src/utils.cu:128-176); a file that cannot be
   // written is reported on stderr and the result is still returned, as the
-  // reference does.
+  // reference does.  Like the reference, every call with N > 0 appends its
+  // row to zeus_<D>d_results.tsv in the working directory and prints the
+  // census line.
   template <typename Function, std::size_t ZEUS_DIM = FnTraits<Function>::arity>
     requires ZeusObjective<Function, ZEUS_DIM>
   Result<ZEUS_DIM>
@@ -368,15 +370,17 @@ namespace zeus {
     (void)parallel;
     (void)prng_type;
     (void)nzerosteps;
-    (void)run;
     constexpr std::size_t D = ZEUS_DIM;
     Result<D> best;
     if (N == 0)
       return best; // zeus.cuh:58-60
     detail::DeviceBuffers b;
-    cudaEvent_t e0, e1;
+    cudaEvent_t e0, e1, p0, p1, p2;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    cudaEventCreate(&p0);
+    cudaEventCreate(&p1);
+    cudaEventCreate(&p2);
     try {
       const int64_t n = (int64_t)N;
       double* starts = b.alloc<double>(N * D);
@@ -398,15 +402,18 @@ namespace zeus {
         w.counter = b.alloc<unsigned int>(1);
         w.gbest = b.alloc<double>(D + 1);
         double* pbf = b.alloc<double>(N);
+        cudaEventRecord(p0, b.st);
         zb::pso_reset_kernel<(int)D><<<1, 256, 0, b.st>>>(w);
         zb::pso_init_kernel<Function, (int)D>
           <<<(unsigned)blocks, zb::kPsoBlock, 0, b.st>>>(f, n, lower, upper,
                                                          (uint64_t)seed, w,
                                                          starts, pbf);
+        cudaEventRecord(p1, b.st);
         for (int t = 1; t <= PSO_ITER; ++t)
           zb::pso_iter_kernel<Function, (int)D>
             <<<(unsigned)blocks, zb::kPsoBlock, 0, b.st>>>(
               f, n, 0.5, 1.2, 1.5, (uint64_t)seed, t, w, starts, pbf);
+        cudaEventRecord(p2, b.st);
       } else if (zeus_starts_uniform((uint64_t)seed, n, (int32_t)D, lower, upper,
                                      starts, b.st) != ZEUS_OK) {
         throw cudaErrorLaunchFailure;
@@ -490,12 +497,34 @@ namespace zeus {
                    cudaMemcpyDeviceToHost);
         best.idx = i;
       }
+      // the reference's per-call results row and census line
+      // (zeus.cuh:170-183, util.hpp:79-136)
+      float ms_init = 0.f, ms_pso = 0.f;
+      if (PSO_ITER >= 0) {
+        cudaEventElapsedTime(&ms_init, p0, p1);
+        cudaEventElapsedTime(&ms_pso, p1, p2);
+      }
+      const std::string fn(fun_name);
+      const double err = zeus_euclidean_error(fn.c_str(), best.coordinates, (int32_t)D);
+      const zeus_result zr{best.idx, best.status, best.fval, best.gradientNorm,
+                           best.iter, 0};
+      const zeus_census zc{hc.actual, hc.claimed, hc.surrendered, hc.stopped,
+                           hc.best_idx, 0};
+      if (zeus_append_results_tsv(nullptr, fn.c_str(), run, n, (int32_t)D, ms_init,
+                                  ms_pso, ms, 0.f, MAX_ITER, PSO_ITER, err, &zr, &zc,
+                                  best.coordinates, nullptr) != ZEUS_OK)
+        std::fprintf(stderr, "Error: %s\n", zeus_last_error());
+      std::printf("claimed: %d\tactual : %d\tsurrendered: %d\tstopped: %d\n",
+                  hc.claimed, hc.actual, hc.surrendered, hc.stopped);
     } catch (cudaError_t e) { // zeus.cuh:112-116: 3 allocation, 4 runtime
       best = Result<D>{};
       best.status = (e == cudaErrorMemoryAllocation) ? 3 : 4;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    cudaEventDestroy(p0);
+    cudaEventDestroy(p1);
+    cudaEventDestroy(p2);
     return best;
   }
 

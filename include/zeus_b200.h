@@ -317,6 +317,29 @@ int zeus_write_trajectory_tsv(const char* path, const double* coords,
                               const int8_t* status, const double* alpha,
                               int64_t n, int32_t max_iter, int32_t dim);
 
+/* ---- the per-call results file ---------------------------------------
+ * Replaces util::calculateEuclideanError (src/util.cpp:12-41): distance of
+ * x from the known minimum by function name -- (1, ..., 1) for
+ * "rosenbrock", (0, -1) for "goldstein_price" (dim 2 only, else NaN), the
+ * origin otherwise. */
+double zeus_euclidean_error(const char* fun_name, const double* x, int32_t dim);
+/* Replaces util::appendResultsToTsv (src/util.cpp:44-108), which every
+ * zeus::Zeus call runs: appends one row to zeus_<dim>d_results.tsv in
+ * `dir` (NULL or "": the current directory), writing the reference's header
+ * first when the file is new or empty.  Columns and number formats are the
+ * reference's: times and metrics as %g, error / fval / norm / coordinates
+ * as %e; `time` is ms_init + ms_pso + ms_opt + ms_rand when pso_iter > 0,
+ * else ms_opt + ms_rand.  `metrics` holds the AD then BFGS
+ * {ms_per_call, calls_per_thread_mean, fraction_of_thread, block95,
+ * serialized} (10 doubles) or NULL for zeros: this library does not sample
+ * per-call cycle counts. */
+int zeus_append_results_tsv(const char* dir, const char* fun_name, int32_t run,
+                            int64_t n, int32_t dim, float ms_init, float ms_pso,
+                            float ms_opt, float ms_rand, int32_t max_iter,
+                            int32_t pso_iter, double error,
+                            const zeus_result* best, const zeus_census* census,
+                            const double* coords, const double* metrics);
+
 /* ---- measurement ----------------------------------------------------
  * No counterpart in the reference: a roofline probe.  Runs `iters`
  * iterations of 8 independent FP64 FMA chains per thread on a grid sized to

@@ -13,17 +13,22 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.fixture(scope="module")
-def traj_path(tmp_path_factory):
-    return tmp_path_factory.mktemp("dropin") / "traj.tsv"
+def workdir(tmp_path_factory):
+    return tmp_path_factory.mktemp("dropin")
 
 
 @pytest.fixture(scope="module")
-def results(cuda, traj_path):
+def traj_path(workdir):
+    return workdir / "traj.tsv"
+
+
+@pytest.fixture(scope="module")
+def results(cuda, traj_path, workdir):
     exe = zbuild.DROPIN_BIN
     if not exe.exists():
         pytest.fail(f"{exe} is missing: run zeus_b200/build.py (build_dropin_test)")
     out = subprocess.run([str(exe), str(traj_path)], capture_output=True, text=True,
-                         timeout=300)
+                         timeout=300, cwd=str(workdir))
     assert out.returncode == 0, out.stderr
     return {d["case"]: d for d in (json.loads(l) for l in out.stdout.splitlines()
                                    if l.startswith("{"))}
@@ -82,3 +87,20 @@ def test_cta_layout_from_template(results):
 def test_zero_runs_default_result(results):
     r = results["empty"]
     assert r["status"] == -1 and r["fval"] == 37.0 and r["idx"] == -1
+
+
+def test_results_files_like_the_reference(results, workdir):
+    """Every call with N > 0 appends its row to zeus_<D>d_results.tsv in the
+    working directory (zeus.cuh:170-183, util.hpp:79-136)."""
+    rows = (workdir / "zeus_2d_results.tsv").read_text().splitlines()
+    assert rows[0].startswith("fun\trun\tN\tkernel\t")
+    assert rows[0].endswith("\tcoord_0\tcoord_1")
+    assert len(rows) == 3  # "rosenbrock" and "traj"; the N == 0 call writes nothing
+    for row, case in zip(rows[1:], ("rosenbrock", "traj")):
+        f = row.split("\t")
+        r = results[case]
+        assert f[0] == "rosenbrock" and int(f[19]) == r["status"]
+        assert float(f[24]) == pytest.approx(r["fval"], rel=1e-5, abs=1e-300)
+        assert int(f[14]) == r["claimed"]
+    for d in (16, 8, 4, 40):
+        assert (workdir / f"zeus_{d}d_results.tsv").exists()

@@ -211,7 +211,8 @@ def test_edge_cases(cuda, mode, grad):
 
 # ---- the whole call with host buffers ----------------------------------------
 @pytest.mark.parametrize("mode,grad", [("fast", "adjoint"), ("fast", "dual"), ("exact", "dual")])
-def test_zeus_rosenbrock_end_to_end(cuda, mode, grad):
+def test_zeus_rosenbrock_end_to_end(cuda, mode, grad, tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)  # Zeus appends zeus_2d_results.tsv here
     r = zb.Zeus(zb.Rosenbrock(2), -5.0, 5.0, 1024, 10000, 10, 100, "rosenbrock", 1e-8, 42,
                 0, mode=mode, gradient=grad, per_run=True)
     assert r.status in (1, 2) and r.fval < 1e-10
@@ -220,9 +221,14 @@ def test_zeus_rosenbrock_end_to_end(cuda, mode, grad):
     assert r.c.claimed + r.c.stopped + r.c.surrendered == 1024
     assert (r.per_run_status == 1).sum() == r.c.claimed
     assert r.per_run_fval[r.idx] == r.per_run_fval.min()
+    row = (tmp_path / "zeus_2d_results.tsv").read_text().splitlines()[1].split("\t")
+    assert row[0] == "rosenbrock" and int(row[14]) == r.c.claimed
+    assert int(row[18]) == r.idx and float(row[24]) == pytest.approx(r.fval, abs=1e-300,
+                                                                      rel=1e-5)
 
 
-def test_zeus_gaussian_and_nll_end_to_end(cuda):
+def test_zeus_gaussian_and_nll_end_to_end(cuda, tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)
     r = zb.Zeus(zb.Gaussian(zb.gaussian_matrix(8)), -5.0, 5.0, 256, 1000, 10, 1000,
                 "gaussian", 1e-8, 1, 0)
     assert r.status == 1 and r.fval < 1e-15

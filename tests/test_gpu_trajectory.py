@@ -12,7 +12,8 @@ from tests.test_trajectory_file import reference_tsv
 pytestmark = pytest.mark.gpu
 
 
-def test_zeus_trajectory_file_equals_oracle(cuda, tmp_path):
+def test_zeus_trajectory_file_equals_oracle(cuda, tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)
     n, iters, seed = 12, 60, 42
     path = tmp_path / "rosen.tsv"
     r = zb.Zeus(zb.Rosenbrock(2), -5.0, 5.0, n, iters, -1, 1000, "rosenbrock", 1e-8, seed,
@@ -25,7 +26,8 @@ def test_zeus_trajectory_file_equals_oracle(cuda, tmp_path):
     assert r.idx == best and r.fval == o["fval"][best] and r.status == o["status"][best]
 
 
-def test_zeus_trajectory_file_with_pso_starts(cuda, tmp_path):
+def test_zeus_trajectory_file_with_pso_starts(cuda, tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)
     path = tmp_path / "ras.tsv"
     r = zb.Zeus(zb.Rastrigin(2), -5.12, 5.12, 8, 30, 5, 1000, "rastrigin", 1e-8, 3, 0,
                 trajectory_file=str(path))
@@ -39,7 +41,8 @@ def test_zeus_trajectory_file_with_pso_starts(cuda, tmp_path):
     assert r.status in (0, 1, 5) and np.isfinite(r.fval)
 
 
-def test_zeus_trajectory_file_rejects_netcdf(cuda, tmp_path):
+def test_zeus_trajectory_file_rejects_netcdf(cuda, tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)
     with pytest.raises(zb.ZeusError):
         zb.Zeus(zb.Rosenbrock(2), -5.0, 5.0, 4, 10, -1, 10, "rosenbrock", 1e-8, 1, 0,
                 trajectory_file=str(tmp_path / "t.nc"))

@@ -11,6 +11,7 @@ fallback: if the library is missing or a call fails, an exception is raised.
 from __future__ import annotations
 
 import ctypes as C
+import time
 import dataclasses
 import os
 from pathlib import Path
@@ -167,6 +168,11 @@ SIGNATURES = {
         C.c_int, [C.POINTER(Problem), C.c_int64, C.c_int64, _P, _P, _P, _P, _P]),
     "zeus_write_trajectory_tsv": (
         C.c_int, [C.c_char_p, _P, _P, _P, _P, _P, C.c_int64, C.c_int32, C.c_int32]),
+    "zeus_euclidean_error": (C.c_double, [C.c_char_p, _P, C.c_int32]),
+    "zeus_append_results_tsv": (
+        C.c_int, [C.c_char_p, C.c_char_p, C.c_int32, C.c_int64, C.c_int32, C.c_float,
+                  C.c_float, C.c_float, C.c_float, C.c_int32, C.c_int32, C.c_double,
+                  C.POINTER(CResult), C.POINTER(CCensus), _P, _P]),
     "zeus_autotune": (
         C.c_int,
         [C.POINTER(Problem), C.POINTER(BfgsConfig), C.c_int64, C.c_uint64, C.c_double,
@@ -330,14 +336,21 @@ def Zeus(f: Objective, lower: float, upper: float, N: int, MAX_ITER: int,
     Philox, and the zero-step limit cannot trigger because the reference's
     line search never returns 0 (utils.cuh:395-411).  A ``trajectory_file``
     (``.tsv``) runs the BFGS in exact mode, which records every iteration,
-    and writes the reference's trajectory file (zeus.cuh:62-103, 189-239)."""
-    del parallel, prng, run, nzerosteps, fun_name
+    and writes the reference's trajectory file (zeus.cuh:62-103, 189-239).
+    Like the reference (zeus.cuh:170-183), every call with N > 0 appends its
+    row to zeus_<D>d_results.tsv in the current directory; here the row's
+    `kernel` and `time` are the call's wall time in ms (no separate PSO
+    timing)."""
+    del parallel, prng, nzerosteps
     if N < 0:
         raise ValueError("N must be >= 0")
+    t0 = time.perf_counter()
     if trajectory_file:
-        return _zeus_with_trajectories(f, lower, upper, N, MAX_ITER, PSO_ITER,
-                                       requiredConverged, tolerance, seed,
-                                       trajectory_file, per_run, stream)
+        r = _zeus_with_trajectories(f, lower, upper, N, MAX_ITER, PSO_ITER,
+                                    requiredConverged, tolerance, seed,
+                                    trajectory_file, per_run, stream)
+        _append_results(f, fun_name, run, N, MAX_ITER, PSO_ITER, r, t0)
+        return r
     cfg = make_config(MAX_ITER, requiredConverged, tolerance, mode, gradient)
     best = CResult()
     census = CCensus()
@@ -360,7 +373,25 @@ def Zeus(f: Objective, lower: float, upper: float, N: int, MAX_ITER: int,
         if rc in (E_NOMEM, E_CUDA):
             return r  # status 3 / 4 as the reference reports them
         check(rc)
+    _append_results(f, fun_name, run, N, MAX_ITER, PSO_ITER, r, t0)
     return r
+
+
+def _append_results(f, fun_name, run, N, MAX_ITER, PSO_ITER, r, t0) -> None:
+    """The reference's per-call results row (util::appendResultsToTsv) and
+    its census line on stdout."""
+    if N == 0:
+        return  # the reference returns before its results file (zeus.cuh:58-60)
+    ms = (time.perf_counter() - t0) * 1e3
+    x = np.ascontiguousarray(r.coordinates, dtype=np.float64)
+    err = lib().zeus_euclidean_error(fun_name.encode(), x.ctypes.data, f.dim)
+    best = CResult(r.idx, r.status, r.fval, r.gradientNorm, r.iter, 0)
+    cen = CCensus(r.c.actual, r.c.claimed, r.c.surrendered, r.c.stopped, r.idx, 0)
+    check(lib().zeus_append_results_tsv(None, fun_name.encode(), run, N, f.dim, 0.0, 0.0,
+                                        ms, 0.0, MAX_ITER, PSO_ITER, err, C.byref(best),
+                                        C.byref(cen), x.ctypes.data, None))
+    print(f"claimed: {r.c.claimed}\tactual : {r.c.actual}\tsurrendered: "
+          f"{r.c.surrendered}\tstopped: {r.c.stopped}")
 
 
 def write_trajectory_tsv(path: str, traj: dict, alpha=None) -> None:

@@ -98,3 +98,118 @@ zeus_write_trajectory_tsv(const char* path, const double* coords,
 }
 
 } // extern "C"
+
+// ---- the per-call results file (util::appendResultsToTsv,
+// include/util.hpp:79-136 / src/util.cpp:44-108; error from
+// util::calculateEuclideanError, src/util.cpp:12-41)
+extern "C" {
+
+double
+zeus_euclidean_error(const char* fun_name, const double* x, int32_t dim)
+{
+  if (!x || dim <= 0)
+    return NAN;
+  const std::string name = fun_name ? fun_name : "";
+  double ss = 0.0;
+  if (name == "rosenbrock") {
+    for (int i = 0; i < dim; ++i) {
+      const double d = x[i] - 1.0;
+      ss += d * d;
+    }
+  } else if (name == "goldstein_price") {
+    if (dim != 2)
+      return NAN;
+    const double dx = x[0] - 0.0, dy = x[1] - (-1.0);
+    ss = dx * dx + dy * dy;
+  } else {
+    for (int i = 0; i < dim; ++i)
+      ss += x[i] * x[i];
+  }
+  return std::sqrt(ss);
+}
+
+int
+zeus_append_results_tsv(const char* dir, const char* fun_name, int32_t run,
+                        int64_t n, int32_t dim, float ms_init, float ms_pso,
+                        float ms_opt, float ms_rand, int32_t max_iter,
+                        int32_t pso_iter, double error, const zeus_result* best,
+                        const zeus_census* census, const double* coords,
+                        const double* metrics)
+{
+  if (!best || !census || dim <= 0 || !coords) {
+    set_error("zeus_append_results_tsv: best, census, dim > 0 and coords are required");
+    return ZEUS_E_INVALID;
+  }
+  std::string path = dir && *dir ? std::string(dir) + "/" : std::string();
+  path += "zeus_" + std::to_string(dim) + "d_results.tsv";
+  std::FILE* fp = std::fopen(path.c_str(), "a");
+  if (!fp) {
+    set_error("zeus_append_results_tsv: cannot open %s", path.c_str());
+    return ZEUS_E_INVALID;
+  }
+  std::string out;
+  std::fseek(fp, 0, SEEK_END);
+  if (std::ftell(fp) == 0) { // a new or empty file gets the header
+    out = "fun\trun\tN\tkernel"
+          "\tad_ms_per_call\tad_calls_per_thread_mean\tad_fraction\tad_block95"
+          "\tad_serialized"
+          "\tbfgs_ms_per_call\tbfgs_calls_per_thread_mean\tbfgs_fraction"
+          "\tbfgs_block95\tbfgs_serialized"
+          "\tclaimed\tactual\tsurrender\tstopped\tidx\tstatus\tbfgs_iter"
+          "\tpso_iter\ttime\terror\tfval\tnorm";
+    for (int i = 0; i < dim; ++i)
+      out += "\tcoord_" + std::to_string(i);
+    out += "\n";
+  }
+  char b[64];
+  // the stream's default floating format is %g (precision 6) until
+  // std::scientific switches it to %.6e for error, fval, norm and the
+  // coordinates
+  auto g = [&](double v) {
+    std::snprintf(b, sizeof b, "%g", v);
+    out += b;
+  };
+  auto e = [&](double v) {
+    std::snprintf(b, sizeof b, "%e", v);
+    out += b;
+  };
+  out += std::string(fun_name ? fun_name : "") + "\t" + std::to_string(run) + "\t" +
+         std::to_string(n) + "\t";
+  g(ms_opt);
+  // metrics: AD then BFGS, each {ms_per_call, calls_per_thread_mean,
+  // fraction_of_thread, block95, serialized}; this library does not sample
+  // per-call cycle counts, so its callers pass NULL (zeros)
+  for (int k = 0; k < 10; ++k) {
+    out += "\t";
+    g(metrics ? metrics[k] : 0.0);
+  }
+  out += "\t" + std::to_string(census->claimed) + "\t" + std::to_string(census->actual) +
+         "\t" + std::to_string(census->surrendered) + "\t" +
+         std::to_string(census->stopped) + "\t" + std::to_string(best->idx) + "\t" +
+         std::to_string(best->status) + "\t" + std::to_string(max_iter) + "\t" +
+         std::to_string(pso_iter) + "\t";
+  const double t = pso_iter > 0 ? (double)ms_init + ms_pso + ms_opt + ms_rand
+                                : (double)ms_opt + ms_rand;
+  g(t);
+  out += "\t";
+  e(error);
+  out += "\t";
+  e(best->fval);
+  out += "\t";
+  e(best->gradient_norm);
+  out += "\t";
+  for (int i = 0; i < dim; ++i) {
+    e(coords[i]);
+    if (i < dim - 1)
+      out += "\t";
+  }
+  out += "\n";
+  const bool ok = std::fwrite(out.data(), 1, out.size(), fp) == out.size();
+  if (std::fclose(fp) != 0 || !ok) {
+    set_error("zeus_append_results_tsv: write to %s failed", path.c_str());
+    return ZEUS_E_INVALID;
+  }
+  return ZEUS_OK;
+}
+
+} // extern "C"
