@@ -307,10 +307,22 @@ namespace zeus {
       }
     };
 
+    // hws: for the CTA layout past about D = 160, a device buffer of
+    // cta_h_slices(n) * D * D doubles holding each block's H
+    inline int64_t
+    cta_h_slices(int64_t n)
+    {
+      int dev = 0, sms = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      return n < 2 * (int64_t)sms ? n : 2 * (int64_t)sms;
+    }
+
     template <class F, std::size_t D>
     cudaError_t
     launch_bfgs(const F& f, const zb::BfgsParams& prm, const double* starts,
-                const zb::RunOut& out, zb::Control* ctl, cudaStream_t st)
+                const zb::RunOut& out, zb::Control* ctl, cudaStream_t st,
+                double* hws = nullptr)
     {
       constexpr bool kAdj = zb::HasAdjoint<F>;
       if constexpr (D <= 8) {
@@ -325,7 +337,7 @@ namespace zeus {
         zb::bfgs_tile_kernel<F, (int)D, TS, kAdj>
           <<<grid, zb::kTileBlock, smem, st>>>(f, prm, starts, out, ctl);
       } else {
-        static_assert(D <= 160, "dimensions above 160 are not supported");
+        static_assert(D <= 1024, "dimensions above 1024 are not supported");
         constexpr int B = D <= 64 ? 256 : 512;
         const size_t smem =
           sizeof(double) * zb::cta_smem_doubles<F, (int)D, kAdj>(B);
@@ -336,9 +348,13 @@ namespace zeus {
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, B, smem);
-        const int64_t cap = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
+        int64_t cap = (int64_t)sms * (per_sm > 0 ? per_sm : 1);
+        if constexpr (zb::cta_h_global((int)D, B)) {
+          const int64_t slices = cta_h_slices(prm.n);
+          cap = cap < slices ? cap : slices;
+        }
         k<<<(unsigned)(prm.n < cap ? prm.n : cap), B, smem, st>>>(f, prm, starts,
-                                                                  out, ctl);
+                                                                  out, ctl, hws);
       }
       return cudaGetLastError();
     }
@@ -447,8 +463,11 @@ namespace zeus {
             f, prm, starts, out, reinterpret_cast<zb::Control*>(ctl), scratch);
         e = cudaGetLastError();
       } else {
+        double* hws = nullptr;
+        if constexpr (D > 32 && zb::cta_h_global((int)D, D <= 64 ? 256 : 512))
+          hws = b.alloc<double>((size_t)detail::cta_h_slices(n) * D * D);
         e = detail::launch_bfgs<Function, D>(
-          f, prm, starts, out, reinterpret_cast<zb::Control*>(ctl), b.st);
+          f, prm, starts, out, reinterpret_cast<zb::Control*>(ctl), b.st, hws);
       }
       cudaEventRecord(e1, b.st);
       if (e != cudaSuccess)

@@ -113,6 +113,9 @@ main(int argc, char** argv)
                               1e-8, 9, 0));
   emit("empty", zeus::Zeus(MyRosenbrock{}, -5.0, 5.0, 0, 100, 10, 10, "rosenbrock", 1e-8,
                            42, 0));
+  // past D = 160: the CTA layout keeps H in global memory
+  emit("sphere200", zeus::Zeus(Sphere<200>{}, -5.0, 5.0, 40, 500, 0, 1000, "sphere",
+                               1e-8, 13, 0));
   if (argc > 1) // trajectory file: exact mode, every iteration recorded
     emit("traj", zeus::Zeus(MyRosenbrock{}, -5.0, 5.0, 6, 40, -1, 1000, "rosenbrock",
                             1e-8, 42, 0, true, zeus::PRNGType::XORWOW, argv[1]));

@@ -102,5 +102,13 @@ def test_results_files_like_the_reference(results, workdir):
         assert f[0] == "rosenbrock" and int(f[19]) == r["status"]
         assert float(f[24]) == pytest.approx(r["fval"], rel=1e-5, abs=1e-300)
         assert int(f[14]) == r["claimed"]
-    for d in (16, 8, 4, 40):
+    for d in (16, 8, 4, 40, 200):
         assert (workdir / f"zeus_{d}d_results.tsv").exists()
+
+
+def test_cta_layout_with_h_in_global_memory(results):
+    """D = 200: H (320 KB) does not fit in shared memory; each block streams
+    its own slice of a global workspace."""
+    r = results["sphere200"]
+    assert r["status"] == 1 and r["fval"] < 1e-12
+    assert r["claimed"] == 40

@@ -29,8 +29,9 @@ namespace zb {
       if (layout == ZEUS_LAYOUT_TILE)
         return tile >= 2 && tile <= 32 && !(tile & (tile - 1)) &&
                ((batch_widths(kind, dim) >> __builtin_ctz((unsigned)tile)) & 1u);
-      if (layout == ZEUS_LAYOUT_CTA)
-        return dim >= kBatchCtaMinDim &&
+      if (layout == ZEUS_LAYOUT_CTA) // H in shared memory only
+        return dim >= kBatchCtaMinDim && !cta_h_global(dim, kBatchBlockSmall) &&
+               !cta_h_global(dim, kBatchBlockLarge) &&
                cta_doubles_rt(kind, dim, kBatchBlockSmall) * sizeof(double) <=
                  227 * 1024;
       return false;

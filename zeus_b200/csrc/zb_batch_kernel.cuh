@@ -131,7 +131,7 @@ namespace zb {
         batch_visit(c, [&](auto f) {
           using F = decltype(f);
           constexpr int D = (int)F::arity;
-          if constexpr (D >= kBatchCtaMinDim &&
+          if constexpr (D >= kBatchCtaMinDim && !cta_h_global(D, kBlock) &&
                         sizeof(double) * cta_smem_doubles<F, D, true>(kBlock) <=
                           227 * 1024)
             cta_run<F, D, true, kBlock>(instance_for(f, c, r), sm, prm,

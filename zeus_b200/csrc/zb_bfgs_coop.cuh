@@ -518,17 +518,39 @@ namespace zb {
            (d % 2 == 0 && cta_rows_per_thread(d, block) <= 8);
   }
 
+  // Everything in shared memory but H and the trial points.
+  __host__ __device__ constexpr size_t
+  cta_vec_doubles(int d, int block)
+  {
+    const int q = cta_sweep_q(d, block);
+    return 7 * (size_t)d + 2 * (size_t)q * d + (size_t)d + 64 + kCtaRedDoubles + block;
+  }
+
+  // Past about D = 160 H no longer fits in shared memory beside the vectors
+  // (even with the fewest trial points): it lives in a global-memory slice
+  // per block (D*D doubles, L2-resident for the blocks in flight -- 148
+  // slices of a 256-D H are 78 MB of the 126 MB L2) and the sweep streams
+  // it with the same coalesced 16-byte row accesses.
+  __host__ __device__ constexpr bool
+  cta_h_global(int d, int block)
+  {
+    return !cta_h_in_registers(d, block) &&
+           ((((size_t)d * d + 1) & ~(size_t)1) + cta_vec_doubles(d, block) +
+            (size_t)(block / 32) * d) * sizeof(double) > 227 * 1024;
+  }
+
   // Shared-memory layout (doubles): H[D*D, rounded up to even; none when H
-  // is in registers] | {s,w}[D] | g[2][D] | u[D] | h[D] | x[D] | partial
-  // sums 2*Q*D | trial point D | (group trials) one trial point per trial
-  // group | trial values 2*32 | reductions | scratch blockDim.
+  // is in registers or in global memory] | {s,w}[D] | g[2][D] | u[D] | h[D]
+  // | x[D] | partial sums 2*Q*D | trial point D | (group trials) one trial
+  // point per trial group | trial values 2*32 | reductions | scratch
+  // blockDim.
   __host__ __device__ constexpr size_t
   cta_smem_base_doubles(int d, int block)
   {
-    const int q = cta_sweep_q(d, block);
-    return (cta_h_in_registers(d, block) ? 0 : (((size_t)d * d + 1) & ~(size_t)1)) +
-           7 * (size_t)d +
-           2 * (size_t)q * d + (size_t)d + 64 + kCtaRedDoubles + block;
+    return (cta_h_in_registers(d, block) || cta_h_global(d, block)
+              ? 0
+              : (((size_t)d * d + 1) & ~(size_t)1)) +
+           cta_vec_doubles(d, block);
   }
 
   // Lanes per line-search trial group: the widest of 32, 16, 8 that gives
@@ -586,7 +608,7 @@ namespace zb {
   __device__ __forceinline__ void
   cta_run(const F& f, double* sm, const BfgsParams& prm,
           const double* __restrict__ x0, int64_t run, const RunOut& out,
-          Control* ctl)
+          Control* ctl, double* __restrict__ hglob = nullptr)
   {
     using S = CtaShape<D>;
     constexpr int C = S::C, NCOL = S::NCOL, RV = S::RV;
@@ -603,9 +625,11 @@ namespace zb {
     constexpr bool kColWarp = cta_col_warps(D, kBlock);
     constexpr bool kHReg = cta_h_in_registers(D, kBlock) && !kColWarp;
     constexpr int RQ = cta_rows_per_thread(D, kBlock);
-    double* H = sm;
+    constexpr bool kHGlob = cta_h_global(D, kBlock);
+    // H: shared memory, or this block's global slice `hglob` (16 B aligned)
+    double* H = kHGlob ? hglob : sm;
     // {s_i, w_i} of the deferred update (16 B aligned)
-    double* SW = H + (kHReg || kColWarp ? 0 : ((D * D + 1) & ~1));
+    double* SW = sm + (kHReg || kColWarp || kHGlob ? 0 : ((D * D + 1) & ~1));
     double* gb = SW + 2 * D;    // two gradient slots of D
     double* u = gb + 2 * D;
     double* h = u + D;
@@ -1037,15 +1061,18 @@ namespace zb {
     __syncthreads();
   }
 
+  // `hws`: gridDim.x slices of D*D doubles when cta_h_global(D, kBlock),
+  // else unused.
   template <class F, int D, bool Adjoint, int kBlock>
   __global__ void __launch_bounds__(kBlock)
     bfgs_cta_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
-                    RunOut out, Control* ctl)
+                    RunOut out, Control* ctl, double* __restrict__ hws = nullptr)
   {
     extern __shared__ __align__(16) double sm[];
+    double* hg = hws ? hws + (size_t)blockIdx.x * D * D : nullptr;
     for (int64_t run = blockIdx.x; run < prm.n; run += gridDim.x)
       cta_run<F, D, Adjoint, kBlock>(f, sm, prm, starts + run * D, run, out,
-                                     ctl);
+                                     ctl, hg);
   }
 
 } // namespace zb

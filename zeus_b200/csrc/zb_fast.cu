@@ -42,14 +42,13 @@ namespace zb {
             cta_layout_supported(kind, dim));
   }
 
+  // Only the CTA layout past about D = 160 (H in global memory) needs one.
   size_t
   fast_workspace_bytes(const Objective& o, const zeus_bfgs_config& c,
                        int64_t n)
   {
-    (void)o;
     (void)c;
-    (void)n;
-    return 0;
+    return cta_workspace_bytes(o.dim, n);
   }
 
   int
@@ -57,8 +56,6 @@ namespace zb {
               const BfgsParams& prm, const double* starts, const RunOut& out,
               Control* ctl, void* ws, size_t ws_bytes, cudaStream_t st)
   {
-    (void)ws;
-    (void)ws_bytes;
     if (prm.n <= 0)
       return ZEUS_OK;
     int layout = c.layout, tile = c.tile;
@@ -86,7 +83,7 @@ namespace zb {
       case ZEUS_LAYOUT_CTA:
         if (!cta_layout_supported(o.kind, o.dim))
           break;
-        return launch_cta(o, c, prm, starts, out, ctl, st);
+        return launch_cta(o, c, prm, starts, out, ctl, ws, ws_bytes, st);
       default:
         break;
     }

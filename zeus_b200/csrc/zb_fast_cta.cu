@@ -1,4 +1,6 @@
-// CTA-per-run fast BFGS launcher (D > 32, H in shared memory).
+// CTA-per-run fast BFGS launcher (D > 32; H in shared memory, or past
+// about D = 160 in a global-memory slice per block taken from the caller's
+// workspace).
 #include "zb_bfgs_coop.cuh"
 #include "zb_objective_visit.cuh"
 
@@ -15,10 +17,19 @@ namespace zb {
       return D <= 64 ? 256 : 512;
     }
 
+    // blocks of a global-H launch (and slices of its workspace)
+    int64_t
+    global_h_slices(int64_t n)
+    {
+      const int64_t cap = 2 * (int64_t)sm_count();
+      return n < cap ? n : cap;
+    }
+
     template <class F, int D, bool Adj>
     int
     launch_one(const F& f, const BfgsParams& prm, const double* starts,
-               const RunOut& out, Control* ctl, cudaStream_t st)
+               const RunOut& out, Control* ctl, void* ws, size_t ws_bytes,
+               cudaStream_t st)
     {
       constexpr int B = cta_block<D>();
       const size_t smem = sizeof(double) * cta_smem_doubles<F, D, Adj>(B);
@@ -39,9 +50,21 @@ namespace zb {
         set_error("CTA layout: dim %d does not fit on an SM", D);
         return ZEUS_E_UNSUPPORTED;
       }
-      const int64_t cap = (int64_t)sm_count() * per_sm;
+      int64_t cap = (int64_t)sm_count() * per_sm;
+      double* hws = nullptr;
+      if constexpr (cta_h_global(D, B)) {
+        const int64_t slices = global_h_slices(prm.n);
+        const size_t need = sizeof(double) * (size_t)D * D * (size_t)slices;
+        if (!ws || ws_bytes < need) {
+          set_error("CTA layout at dim %d keeps H in global memory: %zu workspace "
+                    "bytes needed, got %zu", D, need, ws_bytes);
+          return ZEUS_E_WORKSPACE;
+        }
+        hws = static_cast<double*>(ws);
+        cap = cap < slices ? cap : slices;
+      }
       const unsigned grid = (unsigned)(prm.n < cap ? prm.n : cap);
-      kern<<<grid, B, smem, st>>>(f, prm, starts, out, ctl);
+      kern<<<grid, B, smem, st>>>(f, prm, starts, out, ctl, hws);
       return cuda_fail(cudaGetLastError(), "CTA-layout BFGS launch");
     }
   } // namespace
@@ -56,10 +79,21 @@ namespace zb {
     return cta_smem_doubles_rt(dim, b, true) * sizeof(double) <= kSmemLimit;
   }
 
+  size_t
+  cta_workspace_bytes(int dim, int64_t n)
+  {
+    if (dim < kMinCtaDim || n <= 0)
+      return 0;
+    const int b = dim <= 64 ? 256 : 512;
+    return cta_h_global(dim, b)
+             ? sizeof(double) * (size_t)dim * dim * (size_t)global_h_slices(n)
+             : 0;
+  }
+
   int
   launch_cta(const Objective& o, const zeus_bfgs_config& c,
              const BfgsParams& prm, const double* starts, const RunOut& out,
-             Control* ctl, cudaStream_t st)
+             Control* ctl, void* ws, size_t ws_bytes, cudaStream_t st)
   {
     const bool adjoint = c.gradient == ZEUS_GRAD_ADJOINT;
     return visit_objective(o, [&](auto f) -> int {
@@ -69,8 +103,8 @@ namespace zb {
                     sizeof(double) * cta_smem_doubles_rt(D, cta_block<D>(), true) <=
                       kSmemLimit) {
         if (adjoint)
-          return launch_one<F, D, true>(f, prm, starts, out, ctl, st);
-        return launch_one<F, D, false>(f, prm, starts, out, ctl, st);
+          return launch_one<F, D, true>(f, prm, starts, out, ctl, ws, ws_bytes, st);
+        return launch_one<F, D, false>(f, prm, starts, out, ctl, ws, ws_bytes, st);
       } else {
         set_error("CTA layout: dim %d not built", D);
         return ZEUS_E_UNSUPPORTED;

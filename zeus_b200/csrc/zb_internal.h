@@ -56,7 +56,11 @@ namespace zb {
   bool cta_layout_supported(int kind, int dim);
   int launch_cta(const Objective& o, const zeus_bfgs_config& c,
                  const BfgsParams& prm, const double* starts,
-                 const RunOut& out, Control* ctl, cudaStream_t st);
+                 const RunOut& out, Control* ctl, void* ws, size_t ws_bytes,
+                 cudaStream_t st);
+  // workspace of a CTA-layout launch (non-zero only when H is in global
+  // memory)
+  size_t cta_workspace_bytes(int dim, int64_t n);
   // default layout / tile width for (kind, dim): ZEUS_LAYOUT_* and width
   void default_layout(int kind, int dim, int* layout, int* tile);
 

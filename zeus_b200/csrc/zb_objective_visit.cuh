@@ -8,7 +8,7 @@
 
 namespace zb {
 
-#define ZB_ROSENBROCK_DIMS(X) X(2) X(4) X(8) X(10) X(16) X(32) X(64) X(128)
+#define ZB_ROSENBROCK_DIMS(X) X(2) X(4) X(8) X(10) X(16) X(32) X(64) X(128) X(256)
 #define ZB_RASTRIGIN_DIMS(X) X(2) X(10) X(16)
 #define ZB_ACKLEY_DIMS(X) X(2) X(10) X(30)
 #define ZB_GAUSSIAN_DIMS(X) X(2) X(8) X(32) X(150)
