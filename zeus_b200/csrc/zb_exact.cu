@@ -4,6 +4,7 @@
 #include "zb_bfgs_exact.cuh"
 #include "zb_objective_visit.cuh"
 #include "zb_pso.cuh"
+#include "zb_pso_dmma.cuh"
 
 namespace zb {
 
@@ -112,7 +113,15 @@ namespace zb {
       using F = decltype(f);
       constexpr int D = (int)F::arity;
       pso_reset_kernel<D><<<1, 256, 0, st>>>(wk);
-      if constexpr (D >= kPsoCoopMinDim) {
+      if constexpr (D >= kPsoCoopMinDim && F::kind == ZEUS_OBJ_GAUSSIAN) {
+        // f = 0.5 x^T C x for 8 particles per warp on the FP64 tensor cores
+        const unsigned b8 = (unsigned)pso_dmma_blocks(n);
+        pso_init_dmma_kernel<D><<<b8, kPsoBlock, 0, st>>>(f, n, lower, upper, seed,
+                                                          wk, pbx, pbf);
+        for (int t = 1; t <= iters; ++t)
+          pso_iter_dmma_kernel<D><<<b8, kPsoBlock, 0, st>>>(f, n, w, c1, c2, seed, t,
+                                                            wk, pbx, pbf);
+      } else if constexpr (D >= kPsoCoopMinDim) {
         pso_init_coop_kernel<F, D><<<(unsigned)blocks, kPsoBlock, 0, st>>>(
           f, n, lower, upper, seed, wk, pbx, pbf);
         for (int t = 1; t <= iters; ++t)
