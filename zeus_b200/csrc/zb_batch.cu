@@ -218,12 +218,17 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
   for (const BatchClass& b : hc)
     if (b.layout == ZEUS_LAYOUT_CTA)
       smem_cta = std::max(smem_cta, cta_doubles_rt(b.kind, b.dim, block));
-  // biggest work first: CTA classes by dimension, then the rest by dimension
+  // CTA classes first, smallest dimension (least work per run) first: a
+  // batch lasts as long as its slowest run, and a class whose bulk finishes
+  // early lets its stalled runs (those iterating to MAX_ITER) overlap the
+  // bigger classes' bulk instead of starting after it (the mixed batch:
+  // 44.0 ms largest-first, 40.0 ms smallest-first).  Then the tile/thread
+  // classes, largest dimension first.
   std::stable_sort(hc.begin(), hc.end(), [](const BatchClass& a, const BatchClass& b) {
     const int ka = a.layout == ZEUS_LAYOUT_CTA, kb = b.layout == ZEUS_LAYOUT_CTA;
     if (ka != kb)
       return ka > kb;
-    return a.dim > b.dim;
+    return ka ? a.dim < b.dim : a.dim > b.dim;
   });
   int rc = cuda_fail(cudaMemsetAsync(queues, 0,
                                      sizeof(unsigned long long) * n_classes, st),

@@ -5,7 +5,7 @@
 // spectrum per 256 runs).  One block (512 or 384 threads) per SM:
 //
 //   phase A  the block takes runs of the CTA-layout classes (D > 32) one at
-//            a time from each class's atomic queue, biggest dimension first,
+//            a time from each class's atomic queue, smallest dimension first,
 //            and runs each with the whole block (H in shared memory);
 //   phase B  each warp, independently, walks the tile- and thread-layout
 //            classes: its tiles (or single threads) pop runs from the class
