@@ -361,11 +361,13 @@ namespace zeus {
 
   } // namespace detail
 
-  // The reference's entry point (include/zeus.cuh:341-375).  parallel,
-  // prng_type and nzerosteps are accepted for source compatibility: the
-  // layout follows the dimension, starts and PSO draws come from Philox, and
-  // the zero-step limit cannot trigger (the reference's line search never
-  // returns 0, utils.cuh:395-411).  With a trajectory_file (.tsv) the BFGS
+  // The reference's entry point (include/zeus.cuh:341-375).  prng_type
+  // picks the start positions' generator: Philox4x32-10 for XORWOW and
+  // PHILOX, a digitally shifted Sobol' sequence for SOBOL (starts, or the
+  // PSO's initial swarm; velocities and r1/r2 stay on Philox).  parallel and
+  // nzerosteps are accepted for source compatibility: the layout follows the
+  // dimension, and the zero-step limit cannot trigger (the reference's line
+  // search never returns 0, utils.cuh:395-411).  With a trajectory_file (.tsv) the BFGS
   // runs in exact mode, one run per block in the reference's operation
   // order, recording every iteration (N * MAX_ITER steps, as the reference
   // allocates them), and the file is written in the reference's layout
@@ -384,8 +386,10 @@ namespace zeus {
        std::string_view trajectory_file = {}, int nzerosteps = 0)
   {
     (void)parallel;
-    (void)prng_type;
     (void)nzerosteps;
+    const int32_t prng = prng_type == PRNGType::SOBOL    ? ZEUS_PRNG_SOBOL
+                         : prng_type == PRNGType::PHILOX ? ZEUS_PRNG_PHILOX
+                                                         : ZEUS_PRNG_XORWOW;
     constexpr std::size_t D = ZEUS_DIM;
     Result<D> best;
     if (N == 0)
@@ -417,6 +421,9 @@ namespace zeus {
         w.part_idx = b.alloc<int>(blocks);
         w.counter = b.alloc<unsigned int>(1);
         w.gbest = b.alloc<double>(D + 1);
+        if (prng == ZEUS_PRNG_SOBOL &&
+            zeus_sobol_device_table(&w.sobol) != ZEUS_OK)
+          throw cudaErrorLaunchFailure;
         double* pbf = b.alloc<double>(N);
         cudaEventRecord(p0, b.st);
         zb::pso_reset_kernel<(int)D><<<1, 256, 0, b.st>>>(w);
@@ -430,8 +437,8 @@ namespace zeus {
             <<<(unsigned)blocks, zb::kPsoBlock, 0, b.st>>>(
               f, n, 0.5, 1.2, 1.5, (uint64_t)seed, t, w, starts, pbf);
         cudaEventRecord(p2, b.st);
-      } else if (zeus_starts_uniform((uint64_t)seed, n, (int32_t)D, lower, upper,
-                                     starts, b.st) != ZEUS_OK) {
+      } else if (zeus_starts((uint64_t)seed, prng, n, (int32_t)D, lower, upper,
+                             starts, b.st) != ZEUS_OK) {
         throw cudaErrorLaunchFailure;
       }
       zb::BfgsParams prm{n, MAX_ITER, requiredConverged, tolerance, 0};

@@ -100,6 +100,7 @@ typedef struct zeus_bfgs_config {
   int32_t tile;               /* lanes per run for TILE (0 = auto) */
   int32_t block;              /* threads per block (0 = auto) */
   int32_t flags;              /* ZEUS_FLAG_* */
+  int32_t prng;               /* ZEUS_PRNG_*: start positions (zeus_optimize) */
 } zeus_bfgs_config;
 
 /* Per-run outputs, all device pointers; NULL members are not written.
@@ -149,12 +150,39 @@ const char* zeus_version(void);
 /* 1 if (problem kind, dim) has built kernels for (mode, gradient). */
 int zeus_supported(int32_t kind, int32_t dim, int32_t mode, int32_t gradient);
 
+/* ---- start-position generators (the reference's PRNGType,
+ * traits.hpp:67-71) ------------------------------------------------------
+ * XORWOW, PHILOX: Philox4x32-10, counter-based, no per-run state (cuRAND's
+ *   XORWOW, the reference's default, is not reproduced; Philox takes its
+ *   place).
+ * SOBOL: start positions (and the PSO's initial swarm) are points of a
+ *   Sobol' sequence, run i = point i, coordinate d = dimension d (d < 1024),
+ *   digitally shifted by the seed: the starts of any 2^m consecutive runs
+ *   are stratified in every coordinate.  Velocities and the PSO's r1/r2 stay
+ *   on Philox.  Own direction numbers: primitive polynomials in order of
+ *   degree then value, initial numbers from a fixed splitmix64 stream. */
+#define ZEUS_PRNG_XORWOW 0
+#define ZEUS_PRNG_PHILOX 1
+#define ZEUS_PRNG_SOBOL 2
+
 /* ---- starts ---------------------------------------------------------
- * Uniform starts in [lower, upper) from Philox4x32-10, counter = run index:
- * d_out[i*dim+d].  Replaces the reference's in-kernel cuRAND draws when
- * PSO is off (bfgs_sequential.cuh:73-77, utils.cuh:353-358). */
+ * Starts in [lower, upper): d_out[i*dim+d] = lower + (upper - lower) * u
+ * with u from the generator `prng`, run index i.  Replaces the reference's
+ * in-kernel cuRAND draws when PSO is off (bfgs_sequential.cuh:73-77,
+ * utils.cuh:353-358).  The first SOBOL call on a device copies the direction
+ * table to it (synchronous): make it before any stream capture. */
+int zeus_starts(uint64_t seed, int32_t prng, int64_t n, int32_t dim,
+                double lower, double upper, double* d_out, void* stream);
+/* zeus_starts with ZEUS_PRNG_PHILOX. */
 int zeus_starts_uniform(uint64_t seed, int64_t n, int32_t dim, double lower,
                         double upper, double* d_out, void* stream);
+/* Host copy of the Sobol' direction numbers of dimensions [0, ndim), ndim
+ * <= 1024: out[d*32 + k] = v_{k+1} of dimension d, a 32-bit binary
+ * fraction.  Host only; no device is touched. */
+int zeus_sobol_directions(int32_t ndim, uint32_t* out);
+/* Device address of the full direction table (1024 x 32 uint32) on the
+ * current device, copied there on the first call (synchronous). */
+int zeus_sobol_device_table(const uint32_t** d_table);
 
 /* ---- PSO seeding ----------------------------------------------------
  * Replaces pso::launch (pso.cuh:194-345; kernels 17-155): init plus `iters`
@@ -169,6 +197,15 @@ int zeus_pso_device(const zeus_problem* problem, uint64_t seed, int64_t n,
                     double c1, double c2, double* d_pbest_x,
                     double* d_pbest_f, double* d_gbest, void* d_workspace,
                     size_t workspace_bytes, void* stream);
+/* zeus_pso_device with the initial positions from generator `prng`
+ * (ZEUS_PRNG_*; zeus_pso_device is ZEUS_PRNG_PHILOX), as the reference's
+ * pso::launch takes its cuRAND state type (pso.cuh:194-210). */
+int zeus_pso_device_prng(const zeus_problem* problem, uint64_t seed,
+                         int32_t prng, int64_t n, double lower, double upper,
+                         int32_t iters, double w, double c1, double c2,
+                         double* d_pbest_x, double* d_pbest_f,
+                         double* d_gbest, void* d_workspace,
+                         size_t workspace_bytes, void* stream);
 
 /* No counterpart in the reference (its pso::launch allocates its buffers
  * itself, pso.cuh:211-241).  zeus_pso_device without the workspace, for

@@ -612,6 +612,124 @@ zor_uniform_starts(uint64_t seed, int n, int dim, double lower, double upper,
         lower + (upper - lower) * zor_uniform(seed, 1u, (uint64_t)i, (uint32_t)d);
 }
 
+/* --------------------------------------------------------------- Sobol' */
+/* Sobol' (1967) points with the Bratley-Fox recurrence (ACM TOMS 14 (1988)
+ * 88-100): for the primitive polynomial x^s + a_1 x^(s-1) + ... + a_(s-1) x
+ * + 1 and m_1..m_s, m_k = 2 a_1 m_(k-1) ^ 4 a_2 m_(k-2) ^ ... ^
+ * 2^(s-1) a_(s-1) m_(k-s+1) ^ 2^s m_(k-s) ^ m_(k-s), and v_k = m_k / 2^k
+ * (here as 32-bit fractions).  Dimension 0 is van der Corput (v_k = 2^-k). */
+void
+zor_sobol_directions(int ndim, const uint32_t* poly, const uint32_t* minit,
+                     int maxdeg, uint32_t* dirs)
+{
+  for (int d = 0; d < ndim; ++d) {
+    uint32_t* v = dirs + (size_t)d * 32;
+    if (d == 0) {
+      for (int k = 1; k <= 32; ++k)
+        v[k - 1] = (uint32_t)1u << (32 - k);
+      continue;
+    }
+    int s = 0;
+    while ((poly[d] >> (s + 1)) != 0u)
+      ++s;
+    uint64_t m[33];
+    for (int k = 1; k <= s; ++k)
+      m[k] = minit[(size_t)d * maxdeg + (k - 1)];
+    for (int k = s + 1; k <= 32; ++k) {
+      uint64_t x = ((uint64_t)1 << s) * m[k - s] ^ m[k - s];
+      for (int i = 1; i < s; ++i) {
+        const uint64_t a = (poly[d] >> (s - i)) & 1u;
+        x ^= a * (((uint64_t)1 << i) * m[k - i]);
+      }
+      m[k] = x;
+    }
+    for (int k = 1; k <= 32; ++k)
+      v[k - 1] = (uint32_t)(m[k] << (32 - k));
+  }
+}
+
+/* Order of x modulo p over GF(2) by repeated multiplication (p of degree s,
+ * constant term 1); p is primitive iff the order is 2^s - 1. */
+static int
+sobol_primitive(uint32_t p, int s)
+{
+  const uint32_t top = (uint32_t)1u << s, full = top - 1u;
+  uint32_t r = 1u;
+  for (uint32_t k = 1; k <= full; ++k) {
+    r <<= 1;
+    if (r & top)
+      r ^= p;
+    if (r == 1u)
+      return k == full;
+  }
+  return 0;
+}
+
+static uint64_t
+sobol_splitmix(uint64_t* st)
+{
+  uint64_t z = (*st += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+/* The product's parameters: polynomials in order of degree then value;
+ * m_k = (bits 32..63 of the k-th splitmix64 output of the stream seeded
+ * 0x5A17B01D + 0x100000001B3 * d) mod 2^k, forced odd. */
+int
+zor_sobol_params(int ndim, uint32_t* poly, uint32_t* minit, int maxdeg)
+{
+  int d = 1;
+  if (ndim > 0)
+    poly[0] = 1u;
+  for (int s = 1; d < ndim; ++s) {
+    if (s > maxdeg || s > 30)
+      return -1;
+    for (uint32_t p = ((uint32_t)1u << s) + 1u; d < ndim && p < ((uint32_t)2u << s);
+         p += 2u) {
+      if (!sobol_primitive(p, s))
+        continue;
+      poly[d] = p;
+      uint64_t st = 0x5A17B01Dull + 0x100000001B3ull * (uint64_t)d;
+      for (int k = 1; k <= s; ++k)
+        minit[(size_t)d * maxdeg + (k - 1)] =
+          ((uint32_t)(sobol_splitmix(&st) >> 32) & (((uint32_t)1u << k) - 1u)) | 1u;
+      ++d;
+    }
+  }
+  return 0;
+}
+
+/* Point `run` (low 32 bits, natural order), coordinate d, XOR-shifted by
+ * word 0 of Philox(counter (d, 0, 4, 0), key seed), at its cell midpoint. */
+double
+zor_sobol01(const uint32_t* dirs, uint64_t seed, uint64_t run, uint32_t d)
+{
+  uint32_t ctr[4] = {d, 0u, 4u, 0u};
+  uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  uint32_t sh[4];
+  zor_philox4x32_10(ctr, key, sh);
+  uint32_t x = sh[0];
+  const uint32_t n = (uint32_t)run;
+  for (int k = 0; k < 32; ++k)
+    if ((n >> k) & 1u)
+      x ^= dirs[(size_t)d * 32 + k];
+  return ((double)x + 0.5) / 4294967296.0;
+}
+
+void
+zor_starts(uint64_t seed, const uint32_t* sobol, int n, int dim, double lower,
+           double upper, double* out)
+{
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < dim; ++d) {
+      const double u = sobol ? zor_sobol01(sobol, seed, (uint64_t)i, (uint32_t)d)
+                             : zor_uniform(seed, 1u, (uint64_t)i, (uint32_t)d);
+      out[(size_t)i * dim + d] = lower + (upper - lower) * u;
+    }
+}
+
 /* ----------------------------------------------------------------- PSO */
 /* pso.cuh:104-119 */
 void
@@ -632,6 +750,16 @@ zor_pso(const zor_objective* o, uint64_t seed, int n, double lower,
         double upper, int iters, double w, double c1, double c2,
         double* pbx, double* pbf, double* gbx, double* gbf)
 {
+  return zor_pso_sobol(o, seed, NULL, n, lower, upper, iters, w, c1, c2, pbx,
+                       pbf, gbx, gbf);
+}
+
+int
+zor_pso_sobol(const zor_objective* o, uint64_t seed, const uint32_t* sobol,
+              int n, double lower, double upper, int iters, double w,
+              double c1, double c2, double* pbx, double* pbf, double* gbx,
+              double* gbf)
+{
   const int dim = o->dim;
   double* X = (double*)malloc(sizeof(double) * (size_t)n * dim);
   double* V = (double*)malloc(sizeof(double) * (size_t)n * dim);
@@ -640,7 +768,8 @@ zor_pso(const zor_objective* o, uint64_t seed, int n, double lower,
   int gidx = -1;
   for (int i = 0; i < n; ++i) {
     for (int d = 0; d < dim; ++d) {
-      double ux = zor_uniform(seed, 2u, (uint64_t)i, (uint32_t)d);
+      double ux = sobol ? zor_sobol01(sobol, seed, (uint64_t)i, (uint32_t)d)
+                        : zor_uniform(seed, 2u, (uint64_t)i, (uint32_t)d);
       double uv = zor_uniform(seed, 3u, (uint64_t)i, (uint32_t)d);
       X[(size_t)i * dim + d] = lower + (upper - lower) * ux;
       V[(size_t)i * dim + d] = -vr + (vr - -vr) * uv;

@@ -84,6 +84,23 @@ double zor_uniform(uint64_t seed, uint32_t tag, uint64_t run, uint32_t index);
 void zor_uniform_starts(uint64_t seed, int n, int dim, double lower,
                         double upper, double* out);
 
+/* Sobol' points (the product's quasi-random starts, PRNGType::SOBOL of
+ * traits.hpp:67-71 in own construction).  Direction numbers of dimensions
+ * [0, ndim): dirs[d*32 + k] = v_(k+1) as a 32-bit fraction, from
+ * polynomials poly[d] (bit i = coefficient of x^i; poly[0] unused) and
+ * initial numbers minit[d*maxdeg + k] = m_(k+1). */
+void zor_sobol_directions(int ndim, const uint32_t* poly,
+                          const uint32_t* minit, int maxdeg, uint32_t* dirs);
+/* The product's polynomials and initial numbers; -1 if maxdeg is too
+ * small for ndim. */
+int zor_sobol_params(int ndim, uint32_t* poly, uint32_t* minit, int maxdeg);
+/* Shifted point `run`, coordinate d, in (0, 1). */
+double zor_sobol01(const uint32_t* dirs, uint64_t seed, uint64_t run,
+                   uint32_t d);
+/* Starts in [lower, upper): Sobol' when sobol != NULL, else Philox tag 1. */
+void zor_starts(uint64_t seed, const uint32_t* sobol, int n, int dim,
+                double lower, double upper, double* out);
+
 /* Synchronous PSO (pso.cuh:17-155 with gBest fixed at iteration boundaries,
  * ties to the lowest index).  Writes the BFGS starts (pBestX, n*dim) and the
  * per-particle best values.  Returns 0. */
@@ -91,6 +108,12 @@ int zor_pso(const zor_objective* o, uint64_t seed, int n, double lower,
             double upper, int iters, double w, double c1, double c2,
             double* pbest_x, double* pbest_f, double* gbest_x,
             double* gbest_f);
+/* zor_pso with the initial positions from Sobol' directions `sobol` (NULL:
+ * Philox, as zor_pso). */
+int zor_pso_sobol(const zor_objective* o, uint64_t seed, const uint32_t* sobol,
+                  int n, double lower, double upper, int iters, double w,
+                  double c1, double c2, double* pbest_x, double* pbest_f,
+                  double* gbest_x, double* gbest_f);
 
 /* One reference PSO step for given r1/r2 (pso.cuh:104-119). */
 void zor_pso_step(int dim, double w, double c1, double c2, const double* r1,

@@ -53,6 +53,15 @@ def oracle():
                               _P, _P, _P, _P]
         L.zor_pso_step.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _P, _P,
                                    _P, _P, _P, _P]
+        L.zor_pso_sobol.argtypes = [C.POINTER(ZorObjective), C.c_uint64, _P, C.c_int,
+                                    C.c_double, C.c_double, C.c_int, C.c_double,
+                                    C.c_double, C.c_double, _P, _P, _P, _P]
+        L.zor_sobol_directions.argtypes = [C.c_int, _P, _P, C.c_int, _P]
+        L.zor_sobol_params.argtypes = [C.c_int, _P, _P, C.c_int]
+        L.zor_sobol01.restype = C.c_double
+        L.zor_sobol01.argtypes = [_P, C.c_uint64, C.c_uint64, C.c_uint32]
+        L.zor_starts.argtypes = [C.c_uint64, _P, C.c_int, C.c_int, C.c_double,
+                                 C.c_double, _P]
         _oracle = L
     return _oracle
 
@@ -133,21 +142,59 @@ def ref_bfgs(*a, **k):
     return run_bfgs(ref().zref_bfgs, *a, **k)
 
 
-def oracle_starts(seed, n, dim, lower, upper):
+PRNG_XORWOW, PRNG_PHILOX, PRNG_SOBOL = 0, 1, 2
+SOBOL_MAXDEG = 16
+
+
+def sobol_params(ndim):
+    """The product's Sobol' polynomials and initial direction numbers."""
+    poly = np.zeros(ndim, dtype=np.uint32)
+    minit = np.zeros((ndim, SOBOL_MAXDEG), dtype=np.uint32)
+    assert oracle().zor_sobol_params(ndim, _p(poly), _p(minit), SOBOL_MAXDEG) == 0
+    return poly, minit
+
+
+def sobol_directions(ndim, poly=None, minit=None):
+    """dirs[d, k] = v_(k+1) of dimension d (32-bit fractions)."""
+    if poly is None:
+        poly, minit = sobol_params(ndim)
+    poly = np.ascontiguousarray(poly, dtype=np.uint32)
+    minit = np.ascontiguousarray(minit, dtype=np.uint32)
+    dirs = np.zeros((ndim, 32), dtype=np.uint32)
+    oracle().zor_sobol_directions(ndim, _p(poly), _p(minit), minit.shape[1], _p(dirs))
+    return dirs
+
+
+_SOBOL_DIRS = {}
+
+
+def _sobol_table(prng, dim):
+    if prng != PRNG_SOBOL:
+        return None
+    if dim not in _SOBOL_DIRS:
+        _SOBOL_DIRS[dim] = sobol_directions(dim)
+    return _SOBOL_DIRS[dim]
+
+
+def oracle_starts(seed, n, dim, lower, upper, prng=PRNG_PHILOX):
     out = np.zeros((n, dim))
-    oracle().zor_uniform_starts(seed, n, dim, lower, upper, _p(out))
+    dirs = _sobol_table(prng, dim)
+    oracle().zor_starts(seed, None if dirs is None else _p(dirs), n, dim, lower, upper,
+                        _p(out))
     return out
 
 
 def oracle_pso(kind, dim, seed, n, lower, upper, iters, w=0.5, c1=1.2, c2=1.5,
-               data=None, idata=None):
+               data=None, idata=None, prng=PRNG_PHILOX):
     o = zobj(kind, dim, data, idata)
     pbx = np.zeros((n, dim))
     pbf = np.zeros(n)
     gbx = np.zeros(dim)
     gbf = np.zeros(1)
-    oracle().zor_pso(C.byref(o), seed, n, lower, upper, iters, w, c1, c2, _p(pbx),
-                     _p(pbf), _p(gbx), _p(gbf))
+    dirs = _sobol_table(prng, dim)
+    oracle().zor_pso_sobol(C.byref(o), seed, None if dirs is None else _p(dirs), n,
+                           lower, upper, iters, w, c1, c2, _p(pbx), _p(pbf), _p(gbx),
+                           _p(gbf))
     return pbx, pbf, gbx, gbf[0]
 
 

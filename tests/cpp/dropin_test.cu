@@ -116,8 +116,15 @@ main(int argc, char** argv)
   // past D = 160: the CTA layout keeps H in global memory
   emit("sphere200", zeus::Zeus(Sphere<200>{}, -5.0, 5.0, 40, 500, 0, 1000, "sphere",
                                1e-8, 13, 0));
+  // Sobol' initial swarm
+  emit("sphere16_sobol", zeus::Zeus(Sphere<16>{}, -5.0, 5.0, 256, 2000, 5, 1000,
+                                    "sphere", 1e-8, 7, 0, true, zeus::PRNGType::SOBOL));
   if (argc > 1) // trajectory file: exact mode, every iteration recorded
     emit("traj", zeus::Zeus(MyRosenbrock{}, -5.0, 5.0, 6, 40, -1, 1000, "rosenbrock",
                             1e-8, 42, 0, true, zeus::PRNGType::XORWOW, argv[1]));
+  if (argc > 2) // the same with Sobol' starts (step 0 of each run is its start)
+    emit("traj_sobol", zeus::Zeus(MyRosenbrock{}, -5.0, 5.0, 6, 40, -1, 1000,
+                                  "rosenbrock", 1e-8, 42, 0, true, zeus::PRNGType::SOBOL,
+                                  argv[2]));
   return 0;
 }

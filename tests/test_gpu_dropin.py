@@ -23,12 +23,17 @@ def traj_path(workdir):
 
 
 @pytest.fixture(scope="module")
-def results(cuda, traj_path, workdir):
+def sobol_traj_path(workdir):
+    return workdir / "traj_sobol.tsv"
+
+
+@pytest.fixture(scope="module")
+def results(cuda, traj_path, sobol_traj_path, workdir):
     exe = zbuild.DROPIN_BIN
     if not exe.exists():
         pytest.fail(f"{exe} is missing: run zeus_b200/build.py (build_dropin_test)")
-    out = subprocess.run([str(exe), str(traj_path)], capture_output=True, text=True,
-                         timeout=300, cwd=str(workdir))
+    out = subprocess.run([str(exe), str(traj_path), str(sobol_traj_path)],
+                         capture_output=True, text=True, timeout=300, cwd=str(workdir))
     assert out.returncode == 0, out.stderr
     return {d["case"]: d for d in (json.loads(l) for l in out.stdout.splitlines()
                                    if l.startswith("{"))}
@@ -52,6 +57,22 @@ def test_trajectory_file_from_the_drop_in(results, traj_path):
         np.testing.assert_allclose(float(r0[2]), f0, rtol=1e-13)
     r = results["traj"]
     assert r["status"] in (0, 1)
+
+
+def test_sobol_starts_from_the_drop_in(results, sobol_traj_path):
+    """PRNGType::SOBOL: step 0 of each run's trajectory is its start, point i
+    of the oracle's shifted Sobol' sequence."""
+    from tests import _oracle as O
+
+    rows = sobol_traj_path.read_text().splitlines()
+    st = O.oracle_starts(42, 6, 2, -5.0, 5.0, prng=O.PRNG_SOBOL)
+    assert not np.array_equal(st, O.oracle_starts(42, 6, 2, -5.0, 5.0))
+    for i in range(6):
+        r0 = rows[1 + 40 * i].split("\t")
+        np.testing.assert_array_equal([float(r0[6]), float(r0[7])], st[i])
+    r = results["sphere16_sobol"]
+    assert r["status"] == 1 and r["gnorm"] < 1e-8
+    np.testing.assert_allclose(r["x"], [0.5] * 16, atol=1e-8)
 
 
 def test_rosenbrock_functor(results):
@@ -95,8 +116,9 @@ def test_results_files_like_the_reference(results, workdir):
     rows = (workdir / "zeus_2d_results.tsv").read_text().splitlines()
     assert rows[0].startswith("fun\trun\tN\tkernel\t")
     assert rows[0].endswith("\tcoord_0\tcoord_1")
-    assert len(rows) == 3  # "rosenbrock" and "traj"; the N == 0 call writes nothing
-    for row, case in zip(rows[1:], ("rosenbrock", "traj")):
+    # "rosenbrock", "traj" and "traj_sobol"; the N == 0 call writes nothing
+    assert len(rows) == 4
+    for row, case in zip(rows[1:], ("rosenbrock", "traj", "traj_sobol")):
         f = row.split("\t")
         r = results[case]
         assert f[0] == "rosenbrock" and int(f[19]) == r["status"]

@@ -11,8 +11,9 @@ fallback: if the library is missing or a call fails, an exception is raised.
 from __future__ import annotations
 
 import ctypes as C
-import time
 import dataclasses
+import enum
+import time
 import os
 from pathlib import Path
 from typing import Optional, Sequence
@@ -33,6 +34,26 @@ MODE_EXACT, MODE_FAST = 0, 1
 GRAD_DUAL, GRAD_ADJOINT = 0, 1
 LAYOUT_AUTO, LAYOUT_THREAD, LAYOUT_TILE, LAYOUT_CTA = 0, 1, 2, 3
 FLAG_NO_FIXED_POINT = 1
+PRNG_XORWOW, PRNG_PHILOX, PRNG_SOBOL = 0, 1, 2
+
+
+class PRNGType(enum.IntEnum):
+    """The reference's PRNGType (traits.hpp:67-71).  XORWOW and PHILOX both
+    draw from Philox4x32-10 here; SOBOL places the starts (and the PSO's
+    initial swarm) on a digitally shifted Sobol' sequence."""
+    XORWOW = PRNG_XORWOW
+    PHILOX = PRNG_PHILOX
+    SOBOL = PRNG_SOBOL
+
+
+def prng_code(prng) -> int:
+    """ZEUS_PRNG_* for a PRNGType, its int value, its name, or None (the
+    reference's default, XORWOW)."""
+    if prng is None:
+        return PRNG_XORWOW
+    if isinstance(prng, str):
+        return int(PRNGType[prng.upper()])
+    return int(PRNGType(int(prng)))
 
 _MODES = {"exact": MODE_EXACT, "fast": MODE_FAST}
 _GRADS = {"dual": GRAD_DUAL, "adjoint": GRAD_ADJOINT}
@@ -68,6 +89,7 @@ class BfgsConfig(C.Structure):
         ("tile", C.c_int32),
         ("block", C.c_int32),
         ("flags", C.c_int32),
+        ("prng", C.c_int32),
     ]
 
 
@@ -129,14 +151,26 @@ SIGNATURES = {
     "zeus_last_error": (C.c_char_p, []),
     "zeus_version": (C.c_char_p, []),
     "zeus_supported": (C.c_int, [C.c_int32] * 4),
+    "zeus_starts": (
+        C.c_int,
+        [C.c_uint64, C.c_int32, C.c_int64, C.c_int32, C.c_double, C.c_double, _P, _P],
+    ),
     "zeus_starts_uniform": (
         C.c_int,
         [C.c_uint64, C.c_int64, C.c_int32, C.c_double, C.c_double, _P, _P],
     ),
+    "zeus_sobol_directions": (C.c_int, [C.c_int32, _P]),
+    "zeus_sobol_device_table": (C.c_int, [C.POINTER(C.c_void_p)]),
     "zeus_pso_workspace_size": (C.c_size_t, [C.c_int64, C.c_int32]),
     "zeus_pso_device": (
         C.c_int,
         [C.POINTER(Problem), C.c_uint64, C.c_int64, C.c_double, C.c_double,
+         C.c_int32, C.c_double, C.c_double, C.c_double, _P, _P, _P, _P,
+         C.c_size_t, _P],
+    ),
+    "zeus_pso_device_prng": (
+        C.c_int,
+        [C.POINTER(Problem), C.c_uint64, C.c_int32, C.c_int64, C.c_double, C.c_double,
          C.c_int32, C.c_double, C.c_double, C.c_double, _P, _P, _P, _P,
          C.c_size_t, _P],
     ),
@@ -319,9 +353,9 @@ class Result:
 
 def make_config(max_iter: int, required: int, tol: float, mode: str = "fast",
                 gradient: str = "adjoint", layout: int = LAYOUT_AUTO, tile: int = 0,
-                block: int = 0, flags: int = 0) -> BfgsConfig:
+                block: int = 0, flags: int = 0, prng=None) -> BfgsConfig:
     return BfgsConfig(max_iter, required, tol, _MODES[mode], _GRADS[gradient],
-                      layout, tile, block, flags)
+                      layout, tile, block, flags, prng_code(prng))
 
 
 def Zeus(f: Objective, lower: float, upper: float, N: int, MAX_ITER: int,
@@ -331,27 +365,30 @@ def Zeus(f: Objective, lower: float, upper: float, N: int, MAX_ITER: int,
          nzerosteps: int = 0, *, mode: str = "fast", gradient: str = "adjoint",
          per_run: bool = False, stream=None) -> Result:
     """The reference's zeus::Zeus on a built-in objective, host buffers in and
-    out.  ``parallel``/``prng``/``nzerosteps`` are accepted for signature
-    compatibility: the layout is chosen by dimension, the generator is
-    Philox, and the zero-step limit cannot trigger because the reference's
-    line search never returns 0 (utils.cuh:395-411).  A ``trajectory_file``
+    out.  ``prng`` (a PRNGType, its name or value; None = XORWOW) picks the
+    start positions' generator: Philox for XORWOW and PHILOX, Sobol' for
+    SOBOL.  ``parallel``/``nzerosteps`` are accepted for signature
+    compatibility: the layout is chosen by dimension, and the zero-step limit
+    cannot trigger because the reference's line search never returns 0
+    (utils.cuh:395-411).  A ``trajectory_file``
     (``.tsv``) runs the BFGS in exact mode, which records every iteration,
     and writes the reference's trajectory file (zeus.cuh:62-103, 189-239).
     Like the reference (zeus.cuh:170-183), every call with N > 0 appends its
     row to zeus_<D>d_results.tsv in the current directory; here the row's
     `kernel` and `time` are the call's wall time in ms (no separate PSO
     timing)."""
-    del parallel, prng, nzerosteps
+    del parallel, nzerosteps
     if N < 0:
         raise ValueError("N must be >= 0")
+    prng = prng_code(prng)
     t0 = time.perf_counter()
     if trajectory_file:
         r = _zeus_with_trajectories(f, lower, upper, N, MAX_ITER, PSO_ITER,
                                     requiredConverged, tolerance, seed,
-                                    trajectory_file, per_run, stream)
+                                    trajectory_file, per_run, stream, prng)
         _append_results(f, fun_name, run, N, MAX_ITER, PSO_ITER, r, t0)
         return r
-    cfg = make_config(MAX_ITER, requiredConverged, tolerance, mode, gradient)
+    cfg = make_config(MAX_ITER, requiredConverged, tolerance, mode, gradient, prng=prng)
     best = CResult()
     census = CCensus()
     bx = np.zeros(f.dim)
@@ -375,6 +412,14 @@ def Zeus(f: Objective, lower: float, upper: float, N: int, MAX_ITER: int,
         check(rc)
     _append_results(f, fun_name, run, N, MAX_ITER, PSO_ITER, r, t0)
     return r
+
+
+def sobol_directions(ndim: int) -> np.ndarray:
+    """The library's Sobol' direction numbers (host): (ndim, 32) uint32,
+    row d = v_1..v_32 of dimension d as 32-bit fractions."""
+    out = np.zeros((ndim, 32), dtype=np.uint32)
+    check(lib().zeus_sobol_directions(ndim, out.ctypes.data))
+    return out
 
 
 def _append_results(f, fun_name, run, N, MAX_ITER, PSO_ITER, r, t0) -> None:
@@ -407,12 +452,12 @@ def write_trajectory_tsv(path: str, traj: dict, alpha=None) -> None:
 
 
 def _zeus_with_trajectories(f, lower, upper, N, MAX_ITER, PSO_ITER, required, tol, seed,
-                            path, per_run, stream) -> "Result":
+                            path, per_run, stream, prng=PRNG_XORWOW) -> "Result":
     """Zeus with a trajectory file: PSO (or uniform) starts, exact-mode BFGS
     recording every iteration, the census, then the file."""
     import torch
 
-    from .device import bfgs_device, census_device, pso_device, starts_uniform
+    from .device import bfgs_device, census_device, pso_device, starts
 
     if not str(path).endswith(".tsv"):
         check(lib().zeus_write_trajectory_tsv(str(path).encode(), None, None, None, None,
@@ -420,10 +465,11 @@ def _zeus_with_trajectories(f, lower, upper, N, MAX_ITER, PSO_ITER, required, to
     if N == 0:
         return Result()
     if PSO_ITER >= 0:
-        starts, _, _ = pso_device(f, seed & 0xFFFFFFFFFFFFFFFF, N, lower, upper, PSO_ITER)
+        x0, _, _ = pso_device(f, seed & 0xFFFFFFFFFFFFFFFF, N, lower, upper, PSO_ITER,
+                              prng=prng)
     else:
-        starts = starts_uniform(seed & 0xFFFFFFFFFFFFFFFF, N, f.dim, lower, upper)
-    r = bfgs_device(f, starts, max_iter=MAX_ITER, required=required, tol=tol,
+        x0 = starts(seed & 0xFFFFFFFFFFFFFFFF, N, f.dim, lower, upper, prng=prng)
+    r = bfgs_device(f, x0, max_iter=MAX_ITER, required=required, tol=tol,
                     mode="exact", gradient="dual", traj=True, stream=stream)
     cen = census_device(r.fval, r.status, r.x, f.dim,
                         np.ones(f.dim) if f.kind == OBJ_ROSENBROCK else None)
@@ -441,12 +487,13 @@ def _zeus_with_trajectories(f, lower, upper, N, MAX_ITER, PSO_ITER, required, to
     return out
 
 
-from .device import (bfgs_device, pso_device, starts_uniform, census_device,  # noqa: E402
-                     batch_device, autotune, BatchJob)
+from .device import (bfgs_device, pso_device, starts, starts_uniform,  # noqa: E402
+                     census_device, batch_device, autotune, BatchJob)
 
 __all__ = [
     "Zeus", "write_trajectory_tsv", "Result", "Convergence", "Objective", "Rosenbrock", "Rastrigin",
     "Ackley", "Gaussian", "PoissonNLL", "gaussian_matrix", "bfgs_device",
-    "pso_device", "starts_uniform", "census_device", "lib", "supported",
+    "pso_device", "starts", "starts_uniform", "census_device", "lib", "supported",
+    "PRNGType", "sobol_directions",
     "batch_device", "autotune", "BatchJob",
 ]

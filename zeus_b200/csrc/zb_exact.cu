@@ -87,7 +87,7 @@ namespace zb {
   launch_pso(const Objective& o, uint64_t seed, int64_t n, double lower,
              double upper, int iters, double w, double c1, double c2,
              double* pbx, double* pbf, double* gbest, void* ws,
-             size_t ws_bytes, cudaStream_t st)
+             size_t ws_bytes, cudaStream_t st, const uint32_t* sobol)
   {
     if (n <= 0)
       return ZEUS_OK;
@@ -109,6 +109,7 @@ namespace zb {
     p += align_up(sizeof(int) * (size_t)blocks);
     wk.counter = reinterpret_cast<unsigned int*>(p);
     wk.gbest = gbest;
+    wk.sobol = sobol;
     return visit_objective(o, [&](auto f) -> int {
       using F = decltype(f);
       constexpr int D = (int)F::arity;

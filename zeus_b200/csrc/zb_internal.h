@@ -41,7 +41,8 @@ namespace zb {
   int launch_pso(const Objective& o, uint64_t seed, int64_t n, double lower,
                  double upper, int iters, double w, double c1, double c2,
                  double* pbx, double* pbf, double* gbest, void* ws,
-                 size_t ws_bytes, cudaStream_t st);
+                 size_t ws_bytes, cudaStream_t st,
+                 const uint32_t* sobol = nullptr);
 
   // fast-mode layouts (zb_fast_thread.cu, zb_fast_tile.cu, zb_fast_cta.cu)
   bool thread_layout_supported(int kind, int dim);

@@ -26,6 +26,7 @@
 #include "zb_bfgs_coop.cuh"
 #include "zb_common.cuh"
 #include "zb_philox.cuh"
+#include "zb_sobol.cuh"
 
 namespace zb {
 
@@ -36,6 +37,7 @@ namespace zb {
     int* part_idx;                 // per-block argmin
     unsigned int* counter;         // blocks finished in this launch
     double* gbest;                 // {f, x[D]}
+    const uint32_t* sobol = nullptr; // Sobol' directions: initial positions
   };
 
   inline constexpr int kPsoBlock = 256;
@@ -152,7 +154,7 @@ namespace zb {
       std::array<double, D> xa;
 #pragma unroll 1
       for (int d = 0; d < D; ++d) {
-        const double ux = uniform01(seed, kTagPsoX, (uint64_t)i, (uint32_t)d);
+        const double ux = position01(w.sobol, seed, kTagPsoX, (uint64_t)i, (uint32_t)d);
         const double uv = uniform01(seed, kTagPsoV, (uint64_t)i, (uint32_t)d);
         const double rx = lower + (upper - lower) * ux;
         const double rv = -vr + (vr - -vr) * uv;
@@ -224,7 +226,7 @@ namespace zb {
     if (i < n) { // warp-uniform
       const double vr = (upper - lower) * 0.1;
       for (int d = lane; d < D; d += 32) {
-        const double ux = uniform01(seed, kTagPsoX, (uint64_t)i, (uint32_t)d);
+        const double ux = position01(w.sobol, seed, kTagPsoX, (uint64_t)i, (uint32_t)d);
         const double uv = uniform01(seed, kTagPsoV, (uint64_t)i, (uint32_t)d);
         const double rx = lower + (upper - lower) * ux;
         const double rv = -vr + (vr - -vr) * uv;

@@ -112,7 +112,7 @@ namespace zb {
     for (int e = t; e < cnt * D; e += blockDim.x) {
       const int64_t i = i0 + e / D;
       const int d = e % D;
-      const double ux = uniform01(seed, kTagPsoX, (uint64_t)i, (uint32_t)d);
+      const double ux = position01(w.sobol, seed, kTagPsoX, (uint64_t)i, (uint32_t)d);
       const double uv = uniform01(seed, kTagPsoV, (uint64_t)i, (uint32_t)d);
       const double rx = lower + (upper - lower) * ux;
       const double rv = -vr + (vr - -vr) * uv;

@@ -12,6 +12,7 @@
 #include "zb_internal.h"
 #include "zb_objective_visit.cuh"
 #include "zb_philox.cuh"
+#include "zb_sobol.cuh"
 #include "zb_reduce.cuh"
 
 namespace zb {
@@ -131,7 +132,7 @@ namespace zb {
 
   __global__ void
   starts_kernel(uint64_t seed, int64_t n, int dim, double lower, double upper,
-                double* __restrict__ out)
+                double* __restrict__ out, const uint32_t* __restrict__ sobol)
   {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n * dim)
@@ -140,7 +141,8 @@ namespace zb {
     const int d = (int)(e - i * dim);
     // no contraction: the same bits as lower + (upper - lower) * u in C
     out[e] = __dadd_rn(lower, __dmul_rn(upper - lower,
-                                        uniform01(seed, kTagStarts, (uint64_t)i, d)));
+                                        position01(sobol, seed, kTagStarts,
+                                                   (uint64_t)i, (uint32_t)d)));
   }
 
   __global__ void __launch_bounds__(256)
@@ -187,6 +189,27 @@ namespace zb {
         return ZEUS_E_INVALID;
       }
       return ZEUS_OK;
+    }
+
+    // The Sobol' direction table for generator `prng` on the current
+    // device, or null for the Philox ones.
+    int
+    prng_table(int prng, int dim, const uint32_t** sobol)
+    {
+      *sobol = nullptr;
+      if (prng == ZEUS_PRNG_XORWOW || prng == ZEUS_PRNG_PHILOX)
+        return ZEUS_OK;
+      if (prng != ZEUS_PRNG_SOBOL) {
+        set_error("generator %d is not ZEUS_PRNG_XORWOW, _PHILOX or _SOBOL",
+                  prng);
+        return ZEUS_E_INVALID;
+      }
+      if (dim > kSobolMaxDim) {
+        set_error("Sobol' starts are built for dim <= %d, got %d",
+                  kSobolMaxDim, dim);
+        return ZEUS_E_UNSUPPORTED;
+      }
+      return sobol_table_device(sobol);
     }
 
     Objective
@@ -304,20 +327,32 @@ zeus_supported(int32_t kind, int32_t dim, int32_t mode, int32_t gradient)
 }
 
 int
-zeus_starts_uniform(uint64_t seed, int64_t n, int32_t dim, double lower,
-                    double upper, double* d_out, void* stream)
+zeus_starts(uint64_t seed, int32_t prng, int64_t n, int32_t dim, double lower,
+            double upper, double* d_out, void* stream)
 {
   if (n < 0 || dim <= 0 || (n > 0 && !d_out)) {
-    set_error("zeus_starts_uniform: bad arguments");
+    set_error("zeus_starts: bad arguments");
     return ZEUS_E_INVALID;
   }
+  const uint32_t* sobol = nullptr;
+  int rc = prng_table(prng, dim, &sobol);
+  if (rc)
+    return rc;
   if (n == 0)
     return ZEUS_OK;
   const int64_t total = n * dim;
   const unsigned grid = (unsigned)((total + 255) / 256);
   starts_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(seed, n, dim, lower,
-                                                       upper, d_out);
+                                                       upper, d_out, sobol);
   return cuda_fail(cudaGetLastError(), "starts launch");
+}
+
+int
+zeus_starts_uniform(uint64_t seed, int64_t n, int32_t dim, double lower,
+                    double upper, double* d_out, void* stream)
+{
+  return zeus_starts(seed, ZEUS_PRNG_PHILOX, n, dim, lower, upper, d_out,
+                     stream);
 }
 
 size_t
@@ -335,6 +370,18 @@ zeus_pso_device(const zeus_problem* problem, uint64_t seed, int64_t n,
                 double* d_gbest, void* d_workspace, size_t workspace_bytes,
                 void* stream)
 {
+  return zeus_pso_device_prng(problem, seed, ZEUS_PRNG_PHILOX, n, lower, upper,
+                              iters, w, c1, c2, d_pbest_x, d_pbest_f, d_gbest,
+                              d_workspace, workspace_bytes, stream);
+}
+
+int
+zeus_pso_device_prng(const zeus_problem* problem, uint64_t seed, int32_t prng,
+                     int64_t n, double lower, double upper, int32_t iters,
+                     double w, double c1, double c2, double* d_pbest_x,
+                     double* d_pbest_f, double* d_gbest, void* d_workspace,
+                     size_t workspace_bytes, void* stream)
+{
   int rc = check_problem(problem);
   if (rc)
     return rc;
@@ -342,6 +389,9 @@ zeus_pso_device(const zeus_problem* problem, uint64_t seed, int64_t n,
     set_error("zeus_pso_device: bad arguments");
     return ZEUS_E_INVALID;
   }
+  const uint32_t* sobol = nullptr;
+  if ((rc = prng_table(prng, problem->dim, &sobol)))
+    return rc;
   if (n == 0)
     return ZEUS_OK;
   if (n > 0x7fffffffLL) {
@@ -355,7 +405,8 @@ zeus_pso_device(const zeus_problem* problem, uint64_t seed, int64_t n,
     cudaStreamIsCapturing(st, &cs);
   if (!st || cs != cudaStreamCaptureStatusNone)
     return launch_pso(o, seed, n, lower, upper, iters, w, c1, c2, d_pbest_x,
-                      d_pbest_f, d_gbest, d_workspace, workspace_bytes, st);
+                      d_pbest_f, d_gbest, d_workspace, workspace_bytes, st,
+                      sobol);
   // Capture init + iterations into one graph and launch it.
   rc = cuda_fail(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal),
                  "PSO capture begin");
@@ -363,7 +414,7 @@ zeus_pso_device(const zeus_problem* problem, uint64_t seed, int64_t n,
     return rc;
   const int lrc =
     launch_pso(o, seed, n, lower, upper, iters, w, c1, c2, d_pbest_x,
-               d_pbest_f, d_gbest, d_workspace, workspace_bytes, st);
+               d_pbest_f, d_gbest, d_workspace, workspace_bytes, st, sobol);
   cudaGraph_t graph = nullptr;
   const cudaError_t ec = cudaStreamEndCapture(st, &graph);
   if (lrc) {
@@ -600,14 +651,16 @@ zeus_optimize(const zeus_problem* hp, double lower, double upper, int64_t n,
         (rc = alloc(sizeof(double) * (dim + 1), &gbest)) ||
         (rc = alloc(pws, &pso_ws)))
       return fail(rc);
-    if ((rc = zeus_pso_device(&dp, seed, n, lower, upper, pso_iter, 0.5, 1.2,
-                              1.5, static_cast<double*>(starts),
-                              static_cast<double*>(pbf),
-                              static_cast<double*>(gbest), pso_ws, pws, st)))
+    if ((rc = zeus_pso_device_prng(&dp, seed, cfg.prng, n, lower, upper,
+                                   pso_iter, 0.5, 1.2, 1.5,
+                                   static_cast<double*>(starts),
+                                   static_cast<double*>(pbf),
+                                   static_cast<double*>(gbest), pso_ws, pws,
+                                   st)))
       return fail(rc);
   } else {
-    if ((rc = zeus_starts_uniform(seed, n, dim, lower, upper,
-                                  static_cast<double*>(starts), st)))
+    if ((rc = zeus_starts(seed, cfg.prng, n, dim, lower, upper,
+                          static_cast<double*>(starts), st)))
       return fail(rc);
   }
   const size_t bw = zeus_bfgs_workspace_size(&dp, &cfg, n);

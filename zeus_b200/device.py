@@ -12,7 +12,7 @@ import numpy as np
 import torch
 
 from . import (BatchClass, BfgsConfig, Objective, RunOutputs, check, lib, make_config,
-               LAYOUT_AUTO)
+               prng_code, LAYOUT_AUTO, PRNG_PHILOX)
 
 
 def _stream_handle(stream: Optional[torch.cuda.Stream]) -> int:
@@ -42,6 +42,16 @@ def _as_problem(obj, device):
     return obj if isinstance(obj, DeviceProblem) else DeviceProblem(obj, device)
 
 
+def starts(seed: int, n: int, dim: int, lower: float, upper: float, prng=PRNG_PHILOX,
+           device="cuda", stream=None) -> torch.Tensor:
+    """Starts (n, dim) in [lower, upper) from generator `prng` (a PRNGType,
+    its name or value): Philox uniforms, or Sobol' points for SOBOL."""
+    out = torch.empty((n, dim), dtype=torch.float64, device=device)
+    check(lib().zeus_starts(seed, prng_code(prng), n, dim, lower, upper, _ptr(out),
+                            _stream_handle(stream)))
+    return out
+
+
 def starts_uniform(seed: int, n: int, dim: int, lower: float, upper: float,
                    device="cuda", stream=None) -> torch.Tensor:
     """Philox uniform starts (n, dim) in [lower, upper)."""
@@ -53,8 +63,9 @@ def starts_uniform(seed: int, n: int, dim: int, lower: float, upper: float,
 
 def pso_device(obj, seed: int, n: int, lower: float, upper: float, iters: int,
                w: float = 0.5, c1: float = 1.2, c2: float = 1.5, device="cuda",
-               stream=None):
-    """PSO seeding; returns (pbest_x (n, dim), pbest_f (n,), gbest (dim+1,))."""
+               stream=None, prng=PRNG_PHILOX):
+    """PSO seeding; returns (pbest_x (n, dim), pbest_f (n,), gbest (dim+1,)).
+    `prng` picks the initial positions' generator (Sobol' for SOBOL)."""
     dp = _as_problem(obj, device)
     dim = dp.obj.dim
     pbx = torch.empty((n, dim), dtype=torch.float64, device=device)
@@ -63,9 +74,9 @@ def pso_device(obj, seed: int, n: int, lower: float, upper: float, iters: int,
     wsz = lib().zeus_pso_workspace_size(n, dim)
     ws = torch.empty((max(wsz, 1),), dtype=torch.uint8, device=device)
     prob = dp.c()
-    check(lib().zeus_pso_device(C.byref(prob), seed, n, lower, upper, iters, w,
-                                c1, c2, _ptr(pbx), _ptr(pbf), _ptr(gb), _ptr(ws),
-                                wsz, _stream_handle(stream)))
+    check(lib().zeus_pso_device_prng(C.byref(prob), seed, prng_code(prng), n, lower,
+                                     upper, iters, w, c1, c2, _ptr(pbx), _ptr(pbf),
+                                     _ptr(gb), _ptr(ws), wsz, _stream_handle(stream)))
     return pbx, pbf, gb
 
 
