@@ -64,7 +64,9 @@ def flops_per_grad(kind: int, dim: int, gradient: str, nbins: int = 100) -> floa
         if kind == 2:
             return (2 * T + 6) * dim + 3 * T + 12
         if kind == 3:
-            return 2 * dim * dim + 2 * dim
+            # CTA layout (dim > 32): the accepted trial's value pass formed
+            # C x already; otherwise C x (2 dim^2) and x.(Cx)
+            return 2 * dim if dim > 32 else 2 * dim * dim + 2 * dim
         if kind == 4:
             return (T + 18) * nbins + T + 1
     # dual: dim forward passes of the dual-number body

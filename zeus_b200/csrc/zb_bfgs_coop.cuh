@@ -40,6 +40,10 @@ namespace zb {
     };
   template <class F>
   concept TrialsWithGradient = requires { F::kTrialsWithGradient; };
+  // f(x + a p) = f(x) + a grad f(x).p + a^2 f(p), with value_ctx(grp, x, r)
+  // giving f(x) over a shared scratch vector r (the Gaussian's 0.5 x^T C x)
+  template <class F>
+  concept QuadraticForm = requires { F::kQuadraticForm; };
 
   // f(x) for a shared x, the same value in every member.
   template <class F, int D, class G>
@@ -776,7 +780,37 @@ namespace zb {
         n_eval += found + 1;
       } else {
         double* gt = gb + (cur ^ 1) * D;
-        for (int k = 0; k <= kLineSearchTrials; ++k) {
+        int k0 = 0;
+        if constexpr (QuadraticForm<F>) {
+          // f along the line is best + a ddir + a^2 f(p): one pass over the
+          // objective's data for f(p), then the first passing trial is
+          // found without evaluating f; only that trial is evaluated (it
+          // carries the new gradient), and should its true value fail the
+          // test the search goes on trial by trial from there
+          if (warp == 0) {
+#pragma unroll
+            for (int r = 0; r < RV; ++r) {
+              const int i = lane + 32 * r;
+              if (i < D)
+                xt[i] = pr[r];
+            }
+          }
+          __syncthreads();
+          if (t == 0)
+            stop_now = load_stop(ctl);
+          const double fp = f.value_ctx(grp, xt, gt);
+          ++n_eval;
+          while (k0 < kLineSearchTrials) {
+            const double ak = pow2neg(k0);
+            const double fk = best + ak * fma(ak, fp, ddir);
+            if (fk <= best + kArmijoC1 * ak * ddir && fk < best)
+              break;
+            ++k0;
+          }
+          alpha = pow2neg(k0);
+          __syncthreads(); // xt and gt fully read before the trial writes them
+        }
+        for (int k = k0; k <= kLineSearchTrials; ++k) {
           if (warp == 0) {
 #pragma unroll
             for (int r = 0; r < RV; ++r) {
@@ -786,7 +820,7 @@ namespace zb {
             }
           }
           __syncthreads();
-          if (k == 0 && t == 0)
+          if (k == 0 && t == 0 && !QuadraticForm<F>)
             stop_now = load_stop(ctl);
           double f1;
           if constexpr (kTrialGrad)

@@ -523,6 +523,19 @@ namespace zeus {
       return 0.5 * grp.sum(part);
     }
 
+    // f = 0.5 x.r with r = C^T x formed by ctx_coop into the shared vector
+    // r (the whole group streams C once, coalesced).
+    template <class G>
+    __device__ double
+    value_ctx(const G& grp, const double* x, double* r) const
+    {
+      ctx_coop(grp, x, C, r);
+      double part = 0.0;
+      for (int i = grp.rank(); i < (int)D; i += grp.size())
+        part = fma(x[i], r[i], part);
+      return 0.5 * grp.sum(part);
+    }
+
     // f = 0.5 x.(C^T x); g = C^T x (symmetric C) else (C x + C^T x) / 2.
     // `g` must be shared by the group (it is written by one member per i
     // and read back by all after the final sync).
@@ -530,11 +543,7 @@ namespace zeus {
     __device__ double
     adjoint_coop(const G& grp, const double* x, double* g) const
     {
-      ctx_coop(grp, x, C, g);
-      double part = 0.0;
-      for (int i = grp.rank(); i < (int)D; i += grp.size())
-        part = fma(x[i], g[i], part);
-      const double f = 0.5 * grp.sum(part);
+      const double f = value_ctx(grp, x, g);
       if (!symmetric) {
         // C x = (C^T)^T x: same kernel on the transpose via row reads
         for (int i = grp.rank(); i < (int)D; i += grp.size()) {
@@ -550,6 +559,9 @@ namespace zeus {
     // The value costs the same matrix-vector product as the gradient; the
     // kernels evaluate line-search trials with adjoint_coop and keep g.
     static constexpr bool kTrialsWithGradient = true;
+    // f is a quadratic form: f(x + a p) = f(x) + a grad f(x).p + a^2 f(p)
+    // for every x, p, a, so a line search needs f(p) once, not f per trial.
+    static constexpr bool kQuadraticForm = true;
   };
 
   // Binned Poisson negative log-likelihood of the dijet shape
