@@ -322,7 +322,7 @@ namespace zeus {
     cudaError_t
     launch_bfgs(const F& f, const zb::BfgsParams& prm, const double* starts,
                 const zb::RunOut& out, zb::Control* ctl, cudaStream_t st,
-                double* hws = nullptr)
+                double* hws = nullptr, unsigned long long* queue = nullptr)
     {
       constexpr bool kAdj = zb::HasAdjoint<F>;
       if constexpr (D <= 8) {
@@ -353,8 +353,10 @@ namespace zeus {
           const int64_t slices = cta_h_slices(prm.n);
           cap = cap < slices ? cap : slices;
         }
+        if (queue)
+          cudaMemsetAsync(queue, 0, sizeof *queue, st);
         k<<<(unsigned)(prm.n < cap ? prm.n : cap), B, smem, st>>>(f, prm, starts,
-                                                                  out, ctl, hws);
+                                                                  out, ctl, hws, queue);
       }
       return cudaGetLastError();
     }
@@ -471,10 +473,14 @@ namespace zeus {
         e = cudaGetLastError();
       } else {
         double* hws = nullptr;
-        if constexpr (D > 32 && zb::cta_h_global((int)D, D <= 64 ? 256 : 512))
-          hws = b.alloc<double>((size_t)detail::cta_h_slices(n) * D * D);
+        unsigned long long* queue = nullptr;
+        if constexpr (D > 32) {
+          queue = b.alloc<unsigned long long>(1); // the blocks' run queue
+          if constexpr (zb::cta_h_global((int)D, D <= 64 ? 256 : 512))
+            hws = b.alloc<double>((size_t)detail::cta_h_slices(n) * D * D);
+        }
         e = detail::launch_bfgs<Function, D>(
-          f, prm, starts, out, reinterpret_cast<zb::Control*>(ctl), b.st, hws);
+          f, prm, starts, out, reinterpret_cast<zb::Control*>(ctl), b.st, hws, queue);
       }
       cudaEventRecord(e1, b.st);
       if (e != cudaSuccess)

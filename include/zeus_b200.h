@@ -234,7 +234,10 @@ int zeus_pso_device_noalloc(const zeus_problem* problem, uint64_t seed,
  * line search, update skip, accept-if-better and termination protocol.
  * d_control: 2 int32 {stop flag, converged count}, zeroed by the caller
  * before the first launch (the reference's BFGSContext, context.hpp:7-10).
- * Workspace: zeus_bfgs_workspace_size() bytes (0 for most layouts). */
+ * Workspace: zeus_bfgs_workspace_size() bytes: none for the thread and tile
+ * layouts; the CTA layout (dim > 32) keeps its blocks' run queue there (a
+ * block that finishes a run takes the next unstarted one) and, past about
+ * dim 160, each block's H. */
 size_t zeus_bfgs_workspace_size(const zeus_problem* problem,
                                 const zeus_bfgs_config* config, int64_t n);
 int zeus_bfgs_device(const zeus_problem* problem,

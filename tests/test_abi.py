@@ -89,6 +89,9 @@ def test_workspace_sizes():
     prob = zb.Problem(zb.OBJ_ROSENBROCK, 2, None, None, 0, 0)
     fast = zb.make_config(100, 10, 1e-8, "fast", "adjoint")
     assert L.zeus_bfgs_workspace_size(C.byref(prob), C.byref(fast), 1000) == 0
+    # the CTA layout (dim > 32): its blocks' run queue
+    prob64 = zb.Problem(zb.OBJ_ROSENBROCK, 64, None, None, 0, 0)
+    assert L.zeus_bfgs_workspace_size(C.byref(prob64), C.byref(fast), 1000) == 256
     assert L.zeus_pso_workspace_size(1000, 2) >= 2 * 1000 * 2 * 8
     assert L.zeus_pso_workspace_size(0, 2) == 0
 

@@ -43,7 +43,7 @@ def test_global_h_rejects_a_short_workspace(cuda):
     prob = zb.Problem(zb.OBJ_ROSENBROCK, d, None, None, 0, 0)
     L = zb.lib()
     need = L.zeus_bfgs_workspace_size(C.byref(prob), C.byref(cfg), n)
-    assert need == 8 * d * d * n
+    assert need == 256 + 8 * d * d * n  # the run queue, then one H slice per block
     out = torch.empty((n,), dtype=torch.float64, device="cuda")
     ws = torch.empty((need // 2,), dtype=torch.uint8, device="cuda")
     outs = zb.RunOutputs(out.data_ptr(), None, None, None, None, None, None, None, None, None)

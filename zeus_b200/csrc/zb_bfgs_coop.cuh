@@ -1096,17 +1096,35 @@ namespace zb {
   }
 
   // `hws`: gridDim.x slices of D*D doubles when cta_h_global(D, kBlock),
-  // else unused.
+  // else unused.  `queue` (zeroed before the launch): block b runs run b,
+  // then takes runs gridDim.x, gridDim.x + 1, ... from the counter as it
+  // finishes them, so a long run does not hold back runs statically queued
+  // behind it; without a queue, block b runs b, b + gridDim.x, ...
   template <class F, int D, bool Adjoint, int kBlock>
   __global__ void __launch_bounds__(kBlock)
     bfgs_cta_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
-                    RunOut out, Control* ctl, double* __restrict__ hws = nullptr)
+                    RunOut out, Control* ctl, double* __restrict__ hws = nullptr,
+                    unsigned long long* queue = nullptr)
   {
     extern __shared__ __align__(16) double sm[];
     double* hg = hws ? hws + (size_t)blockIdx.x * D * D : nullptr;
-    for (int64_t run = blockIdx.x; run < prm.n; run += gridDim.x)
+    int64_t run = blockIdx.x;
+    while (run < prm.n) {
       cta_run<F, D, Adjoint, kBlock>(f, sm, prm, starts + run * D, run, out,
                                      ctl, hg);
+      if (!queue) {
+        run += gridDim.x;
+        continue;
+      }
+      // the run's shared memory is dead after its final barrier: the next
+      // index goes through sm[0], fenced by one barrier on each side
+      if (threadIdx.x == 0)
+        reinterpret_cast<long long*>(sm)[0] =
+          (long long)gridDim.x + (long long)atomicAdd(queue, 1ull);
+      __syncthreads();
+      run = reinterpret_cast<const long long*>(sm)[0];
+      __syncthreads();
+    }
   }
 
 } // namespace zb

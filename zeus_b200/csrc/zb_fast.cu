@@ -42,7 +42,8 @@ namespace zb {
             cta_layout_supported(kind, dim));
   }
 
-  // Only the CTA layout past about D = 160 (H in global memory) needs one.
+  // Only the CTA layout needs one: its run queue, and past about D = 160
+  // the blocks' H slices.
   size_t
   fast_workspace_bytes(const Objective& o, const zeus_bfgs_config& c,
                        int64_t n)

@@ -9,6 +9,7 @@ namespace zb {
   namespace {
     constexpr int kMinCtaDim = 33;
     constexpr size_t kSmemLimit = 227 * 1024;
+    constexpr size_t kQueueBytes = 256; // the run queue, ahead of any H slices
 
     template <int D>
     constexpr int
@@ -51,20 +52,24 @@ namespace zb {
         return ZEUS_E_UNSUPPORTED;
       }
       int64_t cap = (int64_t)sm_count() * per_sm;
+      const size_t need = cta_workspace_bytes(D, prm.n);
+      if (!ws || ws_bytes < need) {
+        set_error("CTA layout at dim %d: %zu workspace bytes needed, got %zu", D,
+                  need, ws_bytes);
+        return ZEUS_E_WORKSPACE;
+      }
+      auto* queue = static_cast<unsigned long long*>(ws);
       double* hws = nullptr;
       if constexpr (cta_h_global(D, B)) {
+        hws = reinterpret_cast<double*>(static_cast<char*>(ws) + kQueueBytes);
         const int64_t slices = global_h_slices(prm.n);
-        const size_t need = sizeof(double) * (size_t)D * D * (size_t)slices;
-        if (!ws || ws_bytes < need) {
-          set_error("CTA layout at dim %d keeps H in global memory: %zu workspace "
-                    "bytes needed, got %zu", D, need, ws_bytes);
-          return ZEUS_E_WORKSPACE;
-        }
-        hws = static_cast<double*>(ws);
         cap = cap < slices ? cap : slices;
       }
+      if ((rc = cuda_fail(cudaMemsetAsync(queue, 0, sizeof *queue, st),
+                          "CTA-layout run queue reset")))
+        return rc;
       const unsigned grid = (unsigned)(prm.n < cap ? prm.n : cap);
-      kern<<<grid, B, smem, st>>>(f, prm, starts, out, ctl, hws);
+      kern<<<grid, B, smem, st>>>(f, prm, starts, out, ctl, hws, queue);
       return cuda_fail(cudaGetLastError(), "CTA-layout BFGS launch");
     }
   } // namespace
@@ -85,9 +90,10 @@ namespace zb {
     if (dim < kMinCtaDim || n <= 0)
       return 0;
     const int b = dim <= 64 ? 256 : 512;
-    return cta_h_global(dim, b)
-             ? sizeof(double) * (size_t)dim * dim * (size_t)global_h_slices(n)
-             : 0;
+    return kQueueBytes +
+           (cta_h_global(dim, b)
+              ? sizeof(double) * (size_t)dim * dim * (size_t)global_h_slices(n)
+              : 0);
   }
 
   int
