@@ -1,7 +1,9 @@
 """The Gaussian's line search in the CTA layout: f(x + a p) = f(x) +
-a grad f(x).p + a^2 f(p) for the quadratic form 0.5 x^T C x, so each
-iteration evaluates f(p) once and then only the trial the model accepts
-(which carries the new gradient), instead of one pass over C per trial.
+a grad f(x).p + a^2 f(p) for the quadratic form 0.5 x^T C x.  For symmetric
+C one pass over C per iteration forms C x and C p, decides every trial on
+the model and carries f and g = C x + a C p to the accepted point (exact f
+and g confirm convergence); otherwise f(p) is evaluated once and then only
+the trial the model accepts, instead of one pass over C per trial.
 Checked against the oracle (the reference's algorithm, every trial
 evaluated) on final results and iteration counts, for a symmetric and a
 non-symmetric C, and on the evaluation counters."""
@@ -47,6 +49,8 @@ def test_quadratic_line_search_matches_the_oracle(cuda, dim, symmetric):
     # decisions follow rounding: the reference's own arithmetic takes 13
     # iterations on average there, FMA arithmetic with or without this
     # line search 6.6, run for run the same)
-    # one pass for f(p) and one evaluated trial per iteration, rarely more
+    # two evaluations an iteration, rarely more (symmetric C: C x and C p in
+    # one pass; otherwise f(p) and the accepted trial), plus the start and,
+    # for symmetric C, the exact f and g at the end
     it, ev = got["counters"][:, 0].sum(), got["counters"][:, 1].sum()
-    assert ev <= 2.2 * it + 2 * n
+    assert ev <= 2.2 * it + 3 * n

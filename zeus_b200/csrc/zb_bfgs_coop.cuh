@@ -707,6 +707,31 @@ namespace zb {
       }
     }
     long long n_eval = 1, n_grad = 1;
+    // the symmetric quadratic form carries f and g one step from C x (see
+    // the line search); where a run ends, they are formed exactly at x:
+    // f into fd, ||g|| into gd, g into the current slot
+    const auto exact_at_x = [&](int slot, double& fd, double& gd) {
+      double* gc = gb + slot * D;
+      __syncthreads(); // gc and xcur no longer read
+      if (warp == 0) {
+#pragma unroll
+        for (int r = 0; r < RV; ++r) {
+          const int i = lane + 32 * r;
+          if (i < D)
+            xcur[i] = xr[r];
+        }
+      }
+      __syncthreads();
+      if constexpr (QuadraticForm<F>)
+        fd = f.value_ctx(grp, xcur, gc);
+      double v1[1] = {t < D ? gc[t] * gc[t] : 0.0};
+      grp.template sum<1>(v1);
+      gd = sqrt(v1[0]);
+      ++n_eval;
+    };
+    bool carried = false; // f and g of this run are carried (symmetric quadratic)
+    if constexpr (QuadraticForm<F>)
+      carried = f.symmetric;
     int status = kUnset, iter, executed = -1;
     double fout = best, gout = 0.0;
     bool pend = false; // SW holds an update not yet applied to H
@@ -781,36 +806,98 @@ namespace zb {
       } else {
         double* gt = gb + (cur ^ 1) * D;
         int k0 = 0;
+        bool searched = false;
         if constexpr (QuadraticForm<F>) {
-          // f along the line is best + a ddir + a^2 f(p): one pass over the
-          // objective's data for f(p), then the first passing trial is
-          // found without evaluating f; only that trial is evaluated (it
-          // carries the new gradient), and should its true value fail the
-          // test the search goes on trial by trial from there
-          if (warp == 0) {
+          if (f.symmetric) {
+            // C x and C p in one pass over C: f(x), f(p) and g.p, exact at
+            // this iteration's x, decide every trial; the accepted point's
+            // gradient is g + alpha C p and its value f(x) + alpha g.p +
+            // alpha^2 f(p).  g is formed afresh from C x every iteration,
+            // so these carry one step's rounding, never an accumulation.
+            double* gc = gb + cur * D;
+            if (warp == 0) {
 #pragma unroll
-            for (int r = 0; r < RV; ++r) {
-              const int i = lane + 32 * r;
-              if (i < D)
-                xt[i] = pr[r];
+              for (int r = 0; r < RV; ++r) {
+                const int i = lane + 32 * r;
+                if (i < D) {
+                  xt[i] = pr[r];
+                  xcur[i] = xr[r];
+                }
+              }
             }
+            __syncthreads();
+            if (t == 0)
+              stop_now = load_stop(ctl);
+            f.ctx2_coop(grp, xcur, xt, gc, gt, partU, partH);
+            double v3[3] = {0.0, 0.0, 0.0};
+            if (t < D) {
+              v3[0] = xcur[t] * gc[t];
+              v3[1] = xt[t] * gt[t];
+              v3[2] = gc[t] * xt[t];
+            }
+            grp.template sum<3>(v3);
+            best = 0.5 * v3[0];
+            const double fp = 0.5 * v3[1];
+            ddir = v3[2];
+            n_eval += 2;
+            while (k0 < kLineSearchTrials) {
+              const double ak = pow2neg(k0);
+              const double fk = best + ak * fma(ak, fp, ddir);
+              if (fk <= best + kArmijoC1 * ak * ddir && fk < best)
+                break;
+              ++k0;
+            }
+            alpha = pow2neg(k0);
+            fnew = best + alpha * fma(alpha, fp, ddir);
+            if (t < D) // this thread read gt[t] and gc[t] above, no one else
+              gt[t] = fma(alpha, gt[t], gc[t]);
+            if constexpr (kColWarp) {
+              __syncthreads(); // xt fully read
+              if (warp == 0) {
+#pragma unroll
+                for (int r = 0; r < RV; ++r) {
+                  const int i = lane + 32 * r;
+                  if (i < D)
+                    xt[i] = fma(alpha, pr[r], xr[r]);
+                }
+              }
+            }
+            searched = true;
           }
-          __syncthreads();
-          if (t == 0)
-            stop_now = load_stop(ctl);
-          const double fp = f.value_ctx(grp, xt, gt);
-          ++n_eval;
-          while (k0 < kLineSearchTrials) {
-            const double ak = pow2neg(k0);
-            const double fk = best + ak * fma(ak, fp, ddir);
-            if (fk <= best + kArmijoC1 * ak * ddir && fk < best)
-              break;
-            ++k0;
-          }
-          alpha = pow2neg(k0);
-          __syncthreads(); // xt and gt fully read before the trial writes them
         }
-        for (int k = k0; k <= kLineSearchTrials; ++k) {
+        if constexpr (QuadraticForm<F>) {
+          if (!searched) {
+            // (non-symmetric C: g needs C x and C^T x) f along the line is
+            // best + a ddir + a^2 f(p): one pass over the objective's data
+            // for f(p), then the first passing trial is found without
+            // evaluating f; only that trial is evaluated (it carries the
+            // new gradient), and should its true value fail the test the
+            // search goes on trial by trial from there
+            if (warp == 0) {
+#pragma unroll
+              for (int r = 0; r < RV; ++r) {
+                const int i = lane + 32 * r;
+                if (i < D)
+                  xt[i] = pr[r];
+              }
+            }
+            __syncthreads();
+            if (t == 0)
+              stop_now = load_stop(ctl);
+            const double fp = f.value_ctx(grp, xt, gt);
+            ++n_eval;
+            while (k0 < kLineSearchTrials) {
+              const double ak = pow2neg(k0);
+              const double fk = best + ak * fma(ak, fp, ddir);
+              if (fk <= best + kArmijoC1 * ak * ddir && fk < best)
+                break;
+              ++k0;
+            }
+            alpha = pow2neg(k0);
+            __syncthreads(); // xt and gt fully read before the trial writes them
+          }
+        }
+        for (int k = k0; !searched && k <= kLineSearchTrials; ++k) {
           if (warp == 0) {
 #pragma unroll
             for (int r = 0; r < RV; ++r) {
@@ -1046,11 +1133,19 @@ namespace zb {
         break;
       }
       if (gnrm < prm.tol) {
+        double fd = best, gd = gnrm;
+        if (carried) {
+          // converged on the carried gradient: confirm on the exact one
+          exact_at_x(cur, fd, gd);
+          best = fd;
+          if (!(gd < prm.tol))
+            continue;
+        }
         if (t == 0)
           note_converged(ctl, prm.required);
         status = kConverged;
-        fout = best;
-        gout = gnrm;
+        fout = fd;
+        gout = gd;
         break;
       }
       if (!take && skipped && !(prm.flags & kFlagNoFixedPoint)) {
@@ -1063,11 +1158,15 @@ namespace zb {
       if (status == kUnset)
         status = kSurrender;
       fout = best;
-      double gg = 0.0;
-      const double* g = gb + cur * D;
-      for (int i = lane; i < D; i += 32)
-        gg = fma(g[i], g[i], gg);
-      gout = sqrt(warp_allsum(gg));
+      if (carried) {
+        exact_at_x(cur, fout, gout);
+      } else {
+        double gg = 0.0;
+        const double* g = gb + cur * D;
+        for (int i = lane; i < D; i += 32)
+          gg = fma(g[i], g[i], gg);
+        gout = sqrt(warp_allsum(gg));
+      }
     }
     if (warp == 0 && out.x) {
 #pragma unroll

@@ -500,6 +500,72 @@ namespace zeus {
       grp.sync();
     }
 
+    // rx = C^T x and rp = C^T p in one pass over C: each element of C is
+    // loaded once and feeds two FMAs.  Member t owns column i = t % D and
+    // segment t / D as in ctx_coop; the segments' partial sums meet in the
+    // shared arrays sx and sp (size() doubles each).  Ends with a sync.
+    template <class G>
+    __device__ void
+    ctx2_coop(const G& grp, const double* x, const double* p, double* rx,
+              double* rp, double* sx, double* sp) const
+    {
+      const int t = grp.rank(), nq = grp.size() >= (int)D ? grp.size() / (int)D : 1;
+      const int i = t % (int)D, q = t / (int)D;
+      double ax = 0.0, ap = 0.0;
+      if (q < nq) {
+        double ax1 = 0.0, ap1 = 0.0;
+        int j = q;
+#pragma unroll 8
+        for (; j + nq < (int)D; j += 2 * nq) {
+          const double c0 = C[j * D + i], c1 = C[(j + nq) * D + i];
+          ax = fma(c0, x[j], ax);
+          ap = fma(c0, p[j], ap);
+          ax1 = fma(c1, x[j + nq], ax1);
+          ap1 = fma(c1, p[j + nq], ap1);
+        }
+        if (j < (int)D) {
+          const double c0 = C[j * D + i];
+          ax = fma(c0, x[j], ax);
+          ap = fma(c0, p[j], ap);
+        }
+        ax += ax1;
+        ap += ap1;
+      }
+      if (nq == 1) {
+        // one segment: every member past D idles; members below D loop
+        for (int k = t + grp.size(); k < (int)D; k += grp.size()) {
+          double bx = 0.0, bp = 0.0;
+          for (int jj = 0; jj < (int)D; ++jj) {
+            bx = fma(C[jj * D + k], x[jj], bx);
+            bp = fma(C[jj * D + k], p[jj], bp);
+          }
+          rx[k] = bx;
+          rp[k] = bp;
+        }
+        if (t < (int)D) {
+          rx[t] = ax;
+          rp[t] = ap;
+        }
+        grp.sync();
+        return;
+      }
+      if (q < nq) {
+        sx[q * D + i] = ax;
+        sp[q * D + i] = ap;
+      }
+      grp.sync();
+      if (t < (int)D) {
+        double bx = 0.0, bp = 0.0;
+        for (int k = 0; k < nq; ++k) {
+          bx += sx[k * D + t];
+          bp += sp[k * D + t];
+        }
+        rx[t] = bx;
+        rp[t] = bp;
+      }
+      grp.sync();
+    }
+
     // f alone, 0.5 x.(C^T x): member t forms (C^T x)_i for its columns i
     // (reads of C coalesced across members); used where a whole f is
     // evaluated by a small group (a PSO particle's warp, line-search trial
