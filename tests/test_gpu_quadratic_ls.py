@@ -54,3 +54,37 @@ def test_quadratic_line_search_matches_the_oracle(cuda, dim, symmetric):
     # for symmetric C, the exact f and g at the end
     it, ev = got["counters"][:, 0].sum(), got["counters"][:, 1].sum()
     assert ev <= 2.2 * it + 3 * n
+
+
+def test_unaligned_matrix_takes_the_scalar_pass(cuda):
+    """C 8 bytes off a 16-byte boundary: the pass reads C one double at a
+    time (the pair form needs 16-byte alignment) with the same results up
+    to rounding."""
+    import ctypes as C_
+
+    dim, n = 150, 32
+    Cm = zb.gaussian_matrix(dim)
+    st = O.oracle_starts(23, n, dim, -5.0, 5.0)
+    buf = torch.empty(dim * dim + 1, dtype=torch.float64, device="cuda")
+    buf[1:] = torch.from_numpy(Cm.ravel()).cuda()
+    assert (buf.data_ptr() + 8) % 16 == 8
+    prob = zb.Problem(zb.OBJ_GAUSSIAN, dim, buf.data_ptr() + 8, None, 0,
+                      zb.PROBLEM_SYMMETRIC)
+    cfg = zb.make_config(2000, n + 1, 1e-8, "fast", "adjoint", layout=zb.LAYOUT_CTA)
+    L = zb.lib()
+    wsz = L.zeus_bfgs_workspace_size(C_.byref(prob), C_.byref(cfg), n)
+    ws = torch.empty(max(wsz, 1), dtype=torch.uint8, device="cuda")
+    fval = torch.empty(n, dtype=torch.float64, device="cuda")
+    status = torch.empty(n, dtype=torch.int32, device="cuda")
+    x = torch.empty((n, dim), dtype=torch.float64, device="cuda")
+    outs = zb.RunOutputs(fval.data_ptr(), status.data_ptr(), None, None, x.data_ptr(),
+                         None, None, None, None, None)
+    ctl = torch.zeros(2, dtype=torch.int32, device="cuda")
+    d_st = torch.from_numpy(st).cuda()
+    zb.check(L.zeus_bfgs_device(C_.byref(prob), C_.byref(cfg), d_st.data_ptr(), n,
+                                C_.byref(outs), ctl.data_ptr(), ws.data_ptr(), wsz, None))
+    torch.cuda.synchronize()
+    aligned = _run(Cm, st, 2000)
+    assert (status.cpu().numpy() == 1).all() and (aligned["status"] == 1).all()
+    assert x.abs().max().item() < 1e-9
+    assert fval.abs().max().item() < 1e-17

@@ -502,13 +502,68 @@ namespace zeus {
 
     // rx = C^T x and rp = C^T p in one pass over C: each element of C is
     // loaded once and feeds two FMAs.  Member t owns column i = t % D and
-    // segment t / D as in ctx_coop; the segments' partial sums meet in the
-    // shared arrays sx and sp (size() doubles each).  Ends with a sync.
+    // segment t / D as in ctx_coop (even D: a column pair and segment
+    // t / (D/2)); the segments' partial sums meet in the shared arrays sx
+    // and sp (size() doubles each, 16-byte aligned; the pair form only
+    // where C is 16-byte aligned).  Ends with a sync.
     template <class G>
     __device__ void
     ctx2_coop(const G& grp, const double* x, const double* p, double* rx,
               double* rp, double* sx, double* sp) const
     {
+      constexpr int NP = (int)D / 2;
+      if constexpr (D % 2 == 0) {
+        if (grp.size() >= NP && (reinterpret_cast<uintptr_t>(C) & 15u) == 0) {
+          // even D: member t owns the column pair (2c, 2c+1), c = t % NP,
+          // and segment t / NP, reading C a 16-byte pair at a time
+          const int t = grp.rank(), nq = grp.size() / NP;
+          const int c = t % NP, q = t / NP;
+          double ax0 = 0.0, ax1 = 0.0, ap0 = 0.0, ap1 = 0.0;
+          if (q < nq) {
+            double bx0 = 0.0, bx1 = 0.0, bp0 = 0.0, bp1 = 0.0;
+            const double2* C2 = reinterpret_cast<const double2*>(C) + c;
+            int j = q;
+#pragma unroll 8
+            for (; j + nq < (int)D; j += 2 * nq) {
+              const double2 c0 = C2[j * NP], c1 = C2[(j + nq) * NP];
+              const double x0 = x[j], p0 = p[j], x1 = x[j + nq], p1 = p[j + nq];
+              ax0 = fma(c0.x, x0, ax0);
+              ax1 = fma(c0.y, x0, ax1);
+              ap0 = fma(c0.x, p0, ap0);
+              ap1 = fma(c0.y, p0, ap1);
+              bx0 = fma(c1.x, x1, bx0);
+              bx1 = fma(c1.y, x1, bx1);
+              bp0 = fma(c1.x, p1, bp0);
+              bp1 = fma(c1.y, p1, bp1);
+            }
+            if (j < (int)D) {
+              const double2 c0 = C2[j * NP];
+              ax0 = fma(c0.x, x[j], ax0);
+              ax1 = fma(c0.y, x[j], ax1);
+              ap0 = fma(c0.x, p[j], ap0);
+              ap1 = fma(c0.y, p[j], ap1);
+            }
+            ax0 += bx0;
+            ax1 += bx1;
+            ap0 += bp0;
+            ap1 += bp1;
+            *reinterpret_cast<double2*>(sx + q * D + 2 * c) = make_double2(ax0, ax1);
+            *reinterpret_cast<double2*>(sp + q * D + 2 * c) = make_double2(ap0, ap1);
+          }
+          grp.sync();
+          if (t < (int)D) {
+            double bx = 0.0, bp = 0.0;
+            for (int k = 0; k < nq; ++k) {
+              bx += sx[k * D + t];
+              bp += sp[k * D + t];
+            }
+            rx[t] = bx;
+            rp[t] = bp;
+          }
+          grp.sync();
+          return;
+        }
+      }
       const int t = grp.rank(), nq = grp.size() >= (int)D ? grp.size() / (int)D : 1;
       const int i = t % (int)D, q = t / (int)D;
       double ax = 0.0, ap = 0.0;
