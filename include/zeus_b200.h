@@ -253,7 +253,9 @@ int zeus_bfgs_device(const zeus_problem* problem,
  * runs, starts, outputs and stop-early control, as one Zeus call would --
  * in ONE persistent kernel launch.  Slots are refilled from per-class
  * atomic queues as runs finish; CTA-layout classes (dim > 32) go first,
- * smallest dimension first, then the warp-sized ones.  A class may carry several data instances stored one
+ * smallest dimension first, then the warp-sized ones (one block in 16 takes
+ * the warp-sized ones first).  A class may carry several data instances
+ * stored one
  * after another (Gaussian: dim*dim doubles each; NLL: ndata centres and
  * ndata counts each), run r using instance r / runs_per_instance.
  * Fast mode with adjoint gradients only (config->mode, ->gradient);

@@ -240,6 +240,16 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
   bt.max_iter = config->max_iter;
   bt.tol = config->tolerance;
   bt.flags = config->flags;
+  // With CTA and tile/thread classes together, one block in kEarlyDiv
+  // drains the tile/thread classes first (their bulk is small beside the
+  // CTA classes', and what matters is that their longest runs start early)
+  bool has_cta = false, has_warp = false;
+  for (const BatchClass& b : hc) {
+    has_cta |= b.layout == ZEUS_LAYOUT_CTA;
+    has_warp |= b.layout != ZEUS_LAYOUT_CTA;
+  }
+  constexpr int kEarlyDiv = 16;
+  bt.early_b = has_cta && has_warp ? std::max(1, sm_count() / kEarlyDiv) : 0;
   for (int i = 0; i < n_classes; ++i)
     bt.c[i] = hc[i];
   const size_t smem =

@@ -13,6 +13,11 @@
 //            moment its run converges, stalls or fails.  A warp syncs only
 //            when it moves on to the next class (its tile width may change).
 //
+// Most blocks run phase A, then B.  When a batch has both kinds of class,
+// one block in 16 runs B first, then A: the tile/thread classes' bulk is
+// small, and their few runs that iterate to MAX_ITER then overlap the CTA
+// classes instead of starting after them.
+//
 // The per-run bodies are the standalone layouts' (tile_run, cta_run,
 // thread_run), so results equal the standalone kernels' run for run.
 #pragma once
@@ -52,6 +57,7 @@ namespace zb {
     int max_iter;
     double tol;
     int flags;
+    int early_b; // blocks that drain the tile/thread classes before the CTA ones
     BatchClass c[kMaxBatchClasses];
   };
 

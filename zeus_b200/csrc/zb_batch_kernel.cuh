@@ -114,83 +114,89 @@ namespace zb {
     extern __shared__ __align__(16) double sm[];
     __shared__ unsigned long long sh_run;
 
-    // phase A: CTA-layout classes, one run per block at a time
-    for (int ci = 0; ci < ncls; ++ci) {
-      const BatchClass c = classes[ci];
-      if (c.layout != ZEUS_LAYOUT_CTA)
+    // Blocks below early_b take the tile/thread classes (phase B) before
+    // the CTA ones (phase A): the former's bulk is small, and their few runs
+    // that iterate to MAX_ITER then overlap the CTA classes instead of
+    // starting after them.  The other blocks run A, then B, and find the
+    // tile/thread queues drained or nearly so.
+    const bool early = (int)blockIdx.x < bt.early_b;
+    for (int pass = 0; pass < 2; ++pass) {
+      if ((pass == 0) != early) {
+        // phase A: CTA-layout classes, one run per block at a time
+        for (int ci = 0; ci < ncls; ++ci) {
+          const BatchClass c = classes[ci];
+          if (c.layout != ZEUS_LAYOUT_CTA)
+            continue;
+          const BfgsParams prm{c.n, bt.max_iter, c.required, bt.tol, bt.flags};
+          for (;;) {
+            if (threadIdx.x == 0)
+              sh_run = atomicAdd(c.queue, 1ull);
+            __syncthreads();
+            const int64_t r = (int64_t)sh_run;
+            __syncthreads();
+            if (r >= c.n)
+              break;
+            batch_visit(c, [&](auto f) {
+              using F = decltype(f);
+              constexpr int D = (int)F::arity;
+              if constexpr (D >= kBatchCtaMinDim && !cta_h_global(D, kBlock) &&
+                            sizeof(double) * cta_smem_doubles<F, D, true>(kBlock) <=
+                              227 * 1024)
+                cta_run<F, D, true, kBlock>(instance_for(f, c, r), sm, prm,
+                                                 c.starts + r * D, r, c.out, c.ctl);
+            });
+          }
+        }
+        __syncthreads();
         continue;
-      const BfgsParams prm{c.n, bt.max_iter, c.required, bt.tol, bt.flags};
-      for (;;) {
-        if (threadIdx.x == 0)
-          sh_run = atomicAdd(c.queue, 1ull);
-        __syncthreads();
-        const int64_t r = (int64_t)sh_run;
-        __syncthreads();
-        if (r >= c.n)
-          break;
-        batch_visit(c, [&](auto f) {
-          using F = decltype(f);
-          constexpr int D = (int)F::arity;
-          if constexpr (D >= kBatchCtaMinDim && !cta_h_global(D, kBlock) &&
-                        sizeof(double) * cta_smem_doubles<F, D, true>(kBlock) <=
-                          227 * 1024)
-            cta_run<F, D, true, kBlock>(instance_for(f, c, r), sm, prm,
-                                             c.starts + r * D, r, c.out, c.ctl);
-        });
       }
-    }
-    __syncthreads();
-
-    // phase B: each warp drains the tile / thread classes
-    double* warp_buf = nullptr;
-    {
-      // per-warp buffers follow each other; sized by the host for the
-      // widest class of the batch
-      const int warp = threadIdx.x >> 5;
+      // phase B: each warp drains the tile / thread classes; per-warp
+      // buffers follow each other, sized by the host for the widest class
       size_t stride = 0;
       for (int ci = 0; ci < ncls; ++ci)
         if (classes[ci].layout == ZEUS_LAYOUT_TILE)
           stride = stride > batch_tile_buf_doubles(classes[ci].dim, classes[ci].tile)
                      ? stride
                      : batch_tile_buf_doubles(classes[ci].dim, classes[ci].tile);
-      warp_buf = sm + (size_t)warp * stride;
-    }
-    for (int ci = 0; ci < ncls; ++ci) {
-      const BatchClass c = classes[ci];
-      if (c.layout == ZEUS_LAYOUT_CTA)
-        continue;
-      const BfgsParams prm{c.n, bt.max_iter, c.required, bt.tol, bt.flags};
-      batch_visit(c, [&](auto f) {
-        using F = decltype(f);
-        constexpr int D = (int)F::arity;
-        if (c.layout == ZEUS_LAYOUT_THREAD) {
-          if constexpr (D <= kBatchThreadMaxDim) {
-            for (;;) {
-              const int64_t r = (int64_t)atomicAdd(c.queue, 1ull);
-              if (r >= c.n)
-                break;
-              thread_run<F, D, true>(instance_for(f, c, r), prm,
-                                     c.starts + r * D, r, c.out, c.ctl);
+      double* warp_buf = sm + (size_t)(threadIdx.x >> 5) * stride;
+      for (int ci = 0; ci < ncls; ++ci) {
+        const BatchClass c = classes[ci];
+        if (c.layout == ZEUS_LAYOUT_CTA)
+          continue;
+        const BfgsParams prm{c.n, bt.max_iter, c.required, bt.tol, bt.flags};
+        batch_visit(c, [&](auto f) {
+          using F = decltype(f);
+          constexpr int D = (int)F::arity;
+          if (c.layout == ZEUS_LAYOUT_THREAD) {
+            if constexpr (D <= kBatchThreadMaxDim) {
+              for (;;) {
+                const int64_t r = (int64_t)atomicAdd(c.queue, 1ull);
+                if (r >= c.n)
+                  break;
+                thread_run<F, D, true>(instance_for(f, c, r), prm,
+                                       c.starts + r * D, r, c.out, c.ctl);
+              }
             }
-          }
-        } else if constexpr (D < kBatchCtaMinDim) {
-          constexpr unsigned W = batch_widths(F::kind, D);
-          switch (c.tile) {
+          } else if constexpr (D < kBatchCtaMinDim) {
+            constexpr unsigned W = batch_widths(F::kind, D);
+            switch (c.tile) {
 #define ZB_TS(K)                                                               \
   case (1 << K):                                                               \
     if constexpr ((W >> K) & 1u)                                               \
       drain_tile_class<F, D, (1 << K)>(f, c, prm, warp_buf);                   \
     break;
-            ZB_TS(1)
-            ZB_TS(2)
-            ZB_TS(3)
-            ZB_TS(4)
-            ZB_TS(5)
+              ZB_TS(1)
+              ZB_TS(2)
+              ZB_TS(3)
+              ZB_TS(4)
+              ZB_TS(5)
 #undef ZB_TS
+            }
           }
-        }
-      });
-      __syncwarp();
+        });
+        __syncwarp();
+      }
+      __syncthreads(); // the warp buffers are free again
     }
   }
 
