@@ -100,21 +100,27 @@ def algorithmic_flops(jobs_counters) -> float:
 
 
 # ---------------------------------------------------------------- traffic
-# DRAM bytes (read + write) of one batch-kernel launch, from an ncu capture
-# of the 1/8-size mixed batch (0.543 MB read, 512 B written; the ncu summary
-# for the batch kernel under profiles/), scaled to the full batch by its
-# runs (the bytes are the starts read and the results written, proportional
-# to the runs).
-MEASURED_TRAFFIC = {"mixed": 8 * (542976 + 512)}
+# DRAM bytes (read + write) of one launch of the dominant kernel, from ncu
+# captures summarised under profiles/:
+#  * mixed: the batch kernel on the 1/8-size mixed batch (551 KB read, no
+#    bytes written: the results stay in L2), scaled to the full batch by its
+#    runs (the bytes are the starts read and the results written, in
+#    proportion to the runs);
+#  * gaussian150: the CTA-layout BFGS kernel at full size (1.50 MB read: C,
+#    the starts and the first touch of the outputs).
+MEASURED_TRAFFIC = {
+    "mixed": (8 * 551168, "1/8-size capture x 8"),
+    "gaussian150": (1502208, "full-size capture"),
+}
 
 
 def traffic_of(workload: str) -> dict:
     t = MEASURED_TRAFFIC.get(workload)
     if t is None:
         return {"traffic": None}
-    return {"traffic": t, "traffic_unit": "bytes per launch",
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, 1/8-size "
-                              "capture x 8 (batch-kernel ncu summary under profiles/)"}
+    return {"traffic": t[0], "traffic_unit": "bytes per launch",
+            "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum, {t[1]} "
+                              "(ncu summaries under profiles/)"}
 
 
 # ---------------------------------------------------------------- ranks
