@@ -114,7 +114,8 @@ namespace zb {
       using F = decltype(f);
       constexpr int D = (int)F::arity;
       pso_reset_kernel<D><<<1, 256, 0, st>>>(wk);
-      if constexpr (D >= kPsoCoopMinDim && F::kind == ZEUS_OBJ_GAUSSIAN) {
+      if constexpr (D >= kPsoCoopMinDim && D <= kPsoDmmaMaxDim &&
+                    F::kind == ZEUS_OBJ_GAUSSIAN) {
         // f = 0.5 x^T C x for 8 particles per warp on the FP64 tensor cores
         const unsigned b8 = (unsigned)pso_dmma_blocks(n);
         pso_init_dmma_kernel<D><<<b8, kPsoBlock, 0, st>>>(f, n, lower, upper, seed,

@@ -18,52 +18,66 @@
 namespace zb {
 
   inline constexpr int kPsoDmmaParticles = 8; // per block
+  // the block's positions are staged in static shared memory (8 x D doubles)
+  inline constexpr int kPsoDmmaMaxDim = 512;
 
-  // This warp's share of f for particles i0 .. i0+7 (rows of X; rows >= n
-  // read as 0): the 8-column tiles jt = jt0, jt0 + jstep, ... of Y = X C^T,
-  // each dotted with the same columns of X.  Returns in lane 4r the
-  // partial sum of row r.  Fragment layouts of m8n8k4.f64 (PTX ISA,
-  // "Matrix fragments for mma.m8n8k4 with .f64"): A[lane/4][lane%4],
-  // B[lane%4][lane/4], D[lane/4][2*(lane%4) + {0, 1}].
+  // This warp's share of f for the block's 8 particles, whose positions are
+  // the rows of Xs (shared memory, 8 x D; rows past the swarm are zeros):
+  // the 8-column tiles jt = jt0, jt0 + jstep, ... of Y = X C^T, each dotted
+  // with the same columns of X.  Returns in lane 4r the partial sum of row
+  // r.  Fragment layouts of m8n8k4.f64 (PTX ISA, "Matrix fragments for
+  // mma.m8n8k4 with .f64"): A[lane/4][lane%4], B[lane%4][lane/4],
+  // D[lane/4][2*(lane%4) + {0, 1}].  The MMAs are not volatile, so the
+  // compiler may issue the loads of C several k steps ahead of their use.
   template <int D>
   __device__ __forceinline__ double
-  gauss_f8_dmma_part(const double* __restrict__ C, const double* __restrict__ X,
-                     int64_t i0, int64_t n, int lane, int jt0, int jstep)
+  gauss_f8_dmma_part(const double* __restrict__ C, const double* __restrict__ Xs,
+                     int lane, int jt0, int jstep)
   {
     const int r = lane >> 2, c4 = lane & 3;
-    const int64_t row = i0 + r;
-    const bool rv = row < n;
-    const double* xr = X + (rv ? row : 0) * D;
+    const double* xr = Xs + r * D;
     double acc = 0.0;
     for (int jt = jt0; jt < (D + 7) / 8; jt += jstep) {
       // two accumulator tiles (even and odd k steps): half the chain of
       // dependent MMAs
       double e0 = 0.0, e1 = 0.0, o0 = 0.0, o1 = 0.0;
       const int jb = jt * 8 + r; // the B column (a row of C) this lane loads
-#pragma unroll 4
-      for (int kt = 0; kt < (D + 3) / 4; kt += 2) {
-        const int k = kt * 4 + c4, k2 = k + 4;
-        const double a = (rv && k < D) ? xr[k] : 0.0;
-        const double b = (jb < D && k < D) ? C[(size_t)jb * D + k] : 0.0;
-        const double a2 = (rv && k2 < D) ? xr[k2] : 0.0;
-        const double b2 = (jb < D && k2 < D) ? C[(size_t)jb * D + k2] : 0.0;
-        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 "
-                     "{%0, %1}, {%2}, {%3}, {%0, %1};"
-                     : "+d"(e0), "+d"(e1)
-                     : "d"(a), "d"(b));
-        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 "
-                     "{%0, %1}, {%2}, {%3}, {%0, %1};"
-                     : "+d"(o0), "+d"(o1)
-                     : "d"(a2), "d"(b2));
+      const bool bv = jb < D;
+      const double* cb = C + (size_t)(bv ? jb : 0) * D;
+      // the B operands of up to 40 k steps (D = 150: the whole tile) are
+      // loaded before their MMAs: that many independent loads in flight
+      // instead of one L2 round trip a step
+      constexpr int KT = (D + 3) / 4;
+      constexpr int KC = KT < 40 ? KT : 40;
+      for (int k0 = 0; k0 < KT; k0 += KC) {
+        double bk[KC];
+#pragma unroll
+        for (int kk = 0; kk < KC; ++kk) {
+          const int k = (k0 + kk) * 4 + c4;
+          bk[kk] = (bv && k < D) ? cb[k] : 0.0;
+        }
+#pragma unroll
+        for (int kk = 0; kk < KC; kk += 2) {
+          const int k = (k0 + kk) * 4 + c4, k2 = k + 4;
+          const double a = k < D ? xr[k] : 0.0;
+          const double a2 = (kk + 1 < KC && k2 < D) ? xr[k2] : 0.0;
+          const double b2 = kk + 1 < KC ? bk[kk + 1] : 0.0;
+          asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 "
+              "{%0, %1}, {%2}, {%3}, {%0, %1};"
+              : "+d"(e0), "+d"(e1)
+              : "d"(a), "d"(bk[kk]));
+          asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 "
+              "{%0, %1}, {%2}, {%3}, {%0, %1};"
+              : "+d"(o0), "+d"(o1)
+              : "d"(a2), "d"(b2));
+        }
       }
       const double d0 = e0 + o0, d1 = e1 + o1;
       const int j0 = jt * 8 + c4 * 2;
-      if (rv) {
-        if (j0 < D)
-          acc = fma(xr[j0], d0, acc);
-        if (j0 + 1 < D)
-          acc = fma(xr[j0 + 1], d1, acc);
-      }
+      if (j0 < D)
+        acc = fma(xr[j0], d0, acc);
+      if (j0 + 1 < D)
+        acc = fma(xr[j0 + 1], d1, acc);
     }
     // the four lanes of a row hold its partial sums
     acc += __shfl_xor_sync(0xffffffffu, acc, 1);
@@ -71,17 +85,17 @@ namespace zb {
     return acc;
   }
 
-  // f of the block's 8 particles: every warp takes every 8th column tile;
-  // thread t < 8 returns particle i0 + t's value.  `part` is 8 x 8 doubles
-  // of shared memory.
+  // f of the block's 8 particles (rows of Xs): every warp takes every 8th
+  // column tile; thread t < 8 returns particle t's value.  `part` is 8 x 8
+  // doubles of shared memory.
   template <int D>
   __device__ __forceinline__ double
-  gauss_f8_dmma(const double* __restrict__ C, const double* __restrict__ X, int64_t i0,
-                int64_t n, double* part)
+  gauss_f8_dmma(const double* __restrict__ C, const double* __restrict__ Xs,
+                double* part)
   {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nw = blockDim.x >> 5;
-    const double a = gauss_f8_dmma_part<D>(C, X, i0, n, lane, warp, nw);
+    const double a = gauss_f8_dmma_part<D>(C, Xs, lane, warp, nw);
     if ((lane & 3) == 0)
       part[warp * 8 + (lane >> 2)] = a;
     __syncthreads();
@@ -104,11 +118,15 @@ namespace zb {
                          uint64_t seed, PsoWork w, double* __restrict__ pbx,
                          double* __restrict__ pbf)
   {
+    static_assert(D <= kPsoDmmaMaxDim, "positions staged in static shared memory");
     __shared__ double part[(kPsoBlock / 32) * 8];
+    __shared__ double Xs[kPsoDmmaParticles * D];
     const int t = threadIdx.x;
     const int64_t i0 = (int64_t)blockIdx.x * kPsoDmmaParticles;
     const int64_t cnt = n - i0 < kPsoDmmaParticles ? n - i0 : kPsoDmmaParticles;
     const double vr = (upper - lower) * 0.1;
+    for (int e = (int)cnt * D + t; e < kPsoDmmaParticles * D; e += blockDim.x)
+      Xs[e] = 0.0;
     for (int e = t; e < cnt * D; e += blockDim.x) {
       const int64_t i = i0 + e / D;
       const int d = e % D;
@@ -119,9 +137,10 @@ namespace zb {
       w.X[i * D + d] = rx;
       w.V[i * D + d] = rv;
       pbx[i * D + d] = rx;
+      Xs[e] = rx;
     }
     __syncthreads();
-    const double fv = gauss_f8_dmma<D>(f.C, w.X, i0, n, part);
+    const double fv = gauss_f8_dmma<D>(f.C, Xs, part);
     unsigned long long key = ~0ull;
     int kidx = 0x7fffffff;
     if (t < cnt) {
@@ -138,12 +157,16 @@ namespace zb {
                          uint64_t seed, int t, PsoWork w, double* __restrict__ pbx,
                          double* __restrict__ pbf)
   {
+    static_assert(D <= kPsoDmmaMaxDim, "positions staged in static shared memory");
     __shared__ double part[(kPsoBlock / 32) * 8];
+    __shared__ double Xs[kPsoDmmaParticles * D];
     __shared__ int better[kPsoDmmaParticles];
     const int tid = threadIdx.x;
     const int64_t i0 = (int64_t)blockIdx.x * kPsoDmmaParticles;
     const int64_t cnt = n - i0 < kPsoDmmaParticles ? n - i0 : kPsoDmmaParticles;
     const uint32_t tag = kTagPsoIter + (uint32_t)t;
+    for (int e = (int)cnt * D + tid; e < kPsoDmmaParticles * D; e += blockDim.x)
+      Xs[e] = 0.0;
     for (int e = tid; e < cnt * D; e += blockDim.x) {
       const int64_t i = i0 + e / D;
       const int d = e % D;
@@ -156,9 +179,10 @@ namespace zb {
       const double nv = wi * vi + c1 * r1 * (pb - xi) + c2 * r2 * (gb - xi);
       w.V[i * D + d] = nv;
       w.X[i * D + d] = xi + nv;
+      Xs[e] = xi + nv;
     }
     __syncthreads();
-    const double fv = gauss_f8_dmma<D>(f.C, w.X, i0, n, part);
+    const double fv = gauss_f8_dmma<D>(f.C, Xs, part);
     unsigned long long key = ~0ull;
     int kidx = 0x7fffffff;
     if (tid < kPsoDmmaParticles) {
@@ -175,7 +199,7 @@ namespace zb {
     for (int e = tid; e < cnt * D; e += blockDim.x) {
       const int64_t i = i0 + e / D;
       if (better[e / D])
-        pbx[i * D + e % D] = w.X[i * D + e % D];
+        pbx[i * D + e % D] = Xs[e];
     }
     pso_publish<D>(w, w.X, key, kidx);
   }
