@@ -596,6 +596,23 @@ namespace zb {
     return cta_smem_doubles_rt(D, block, cta_warp_trials<F, Adjoint>());
   }
 
+  // The first line-search trial k (alpha = 2^-k) that passes the
+  // reference's test on the quadratic model f(alpha) = f0 + alpha gp +
+  // alpha^2 fp, else kLineSearchTrials: lane k judges trial k, one ballot
+  // picks the lowest.  Every warp of a block gets the same answer.
+  __device__ __forceinline__ int
+  model_trial(double f0, double gp, double fp, int lane)
+  {
+    bool pass = false;
+    if (lane <= kLineSearchTrials) {
+      const double ak = pow2neg(lane);
+      const double fk = f0 + ak * fma(ak, fp, gp);
+      pass = lane == kLineSearchTrials ||
+             (fk <= f0 + kArmijoC1 * ak * gp && fk < f0);
+    }
+    return __ffs(__ballot_sync(0xffffffffu, pass)) - 1;
+  }
+
   __device__ __forceinline__ double
   warp_allsum(double v)
   {
@@ -840,13 +857,7 @@ namespace zb {
             const double fp = 0.5 * v3[1];
             ddir = v3[2];
             n_eval += 2;
-            while (k0 < kLineSearchTrials) {
-              const double ak = pow2neg(k0);
-              const double fk = best + ak * fma(ak, fp, ddir);
-              if (fk <= best + kArmijoC1 * ak * ddir && fk < best)
-                break;
-              ++k0;
-            }
+            k0 = model_trial(best, ddir, fp, lane);
             alpha = pow2neg(k0);
             fnew = best + alpha * fma(alpha, fp, ddir);
             if (t < D) // this thread read gt[t] and gc[t] above, no one else
@@ -886,13 +897,7 @@ namespace zb {
               stop_now = load_stop(ctl);
             const double fp = f.value_ctx(grp, xt, gt);
             ++n_eval;
-            while (k0 < kLineSearchTrials) {
-              const double ak = pow2neg(k0);
-              const double fk = best + ak * fma(ak, fp, ddir);
-              if (fk <= best + kArmijoC1 * ak * ddir && fk < best)
-                break;
-              ++k0;
-            }
+            k0 = model_trial(best, ddir, fp, lane);
             alpha = pow2neg(k0);
             __syncthreads(); // xt and gt fully read before the trial writes them
           }
