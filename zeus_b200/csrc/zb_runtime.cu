@@ -80,22 +80,41 @@ namespace zb {
         idx = (int)i;
       }
       const int st = status[i];
-      if (st == kConverged) {
+      if (st == kConverged)
         ++claimed;
-        if (x) {
-          double ss = 0.0;
-          for (int d = 0; d < dim; ++d) {
-            const double m = km.has ? km.x[d] : 0.0;
-            const double df = x[i * dim + d] - m;
-            ss += df * df;
-          }
-          if (sqrt(ss) < 0.5)
+      else if (st == kStopped)
+        ++stopped;
+      else
+        ++surr;
+    }
+    if (x) {
+      // converged runs within 0.5 of the known minimum: a warp per run, its
+      // lanes over the coordinates (coalesced rows of x), four runs in flight
+      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      const int nw = blockDim.x >> 5;
+      constexpr int R = 4;
+      for (int64_t i0 = (int64_t)warp * R; i0 < n; i0 += (int64_t)nw * R) {
+        double ss[R];
+        bool conv[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int64_t i = i0 + r;
+          conv[r] = i < n && status[i] == kConverged;
+          ss[r] = 0.0;
+          if (conv[r])
+            for (int d = lane; d < dim; d += 32) {
+              const double df = x[i * dim + d] - (km.has ? km.x[d] : 0.0);
+              ss[r] = fma(df, df, ss[r]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+#pragma unroll
+          for (int m = 16; m > 0; m >>= 1)
+            ss[r] += __shfl_xor_sync(0xffffffffu, ss[r], m);
+          if (lane == 0 && conv[r] && sqrt(ss[r]) < 0.5)
             ++actual;
         }
-      } else if (st == kStopped) {
-        ++stopped;
-      } else {
-        ++surr;
       }
     }
     atomicAdd(&cnt[0], actual);
