@@ -220,7 +220,7 @@ int zeus_pso_device_prng(const zeus_problem* problem, uint64_t seed,
  * stream capture.  All calls share the array and it keeps the last call's
  * contents; each call clears what must start at zero, but calls that
  * overlap on the GPU race on it: serialize them.  Outputs as for
- * zeus_pso_device. */
+ * zeus_pso_device (Philox positions, as ZEUS_PRNG_PHILOX). */
 int zeus_pso_device_noalloc(const zeus_problem* problem, uint64_t seed,
                             int64_t n, double lower, double upper,
                             int32_t iters, double w, double c1, double c2,
