@@ -318,6 +318,44 @@ int zeus_autotune_lookup(int32_t kind, int32_t dim, int32_t gradient,
 int zeus_autotune_record(int32_t kind, int32_t dim, int32_t gradient,
                          int32_t layout, int32_t tile);
 
+/* ---- gradient evaluation ----------------------------------------------
+ * Replaces dual::calculateGradientUsingAD (duals.cuh:241-266) as a call of
+ * its own, for checking every gradient path of the BFGS layouts at given
+ * points: writes f(x_i) to d_f[i] and grad f(x_i) to d_g[i*dim + d] for the
+ * n points d_x[i*dim + d] (row-major), evaluated by the device functions the
+ * BFGS kernels step on.  `gradient` is ZEUS_GRAD_DUAL (the plain form's D
+ * forward dual passes) or ZEUS_GRAD_ADJOINT (the hand-written reverse-mode
+ * gradient); `path` picks the layout:
+ *   THREAD     one thread per point (dim <= 32; the thread layout);
+ *   TILE       a tile of `width` lanes per point, value and gradient in one
+ *              cooperative call (a width zeus_tile_widths reports);
+ *   TILE_GRAD  the tile's gradient-only form (adjoint only; f from the
+ *              cooperative value) -- the form tile_run calls;
+ *   CTA        a block of `width` threads per point (a multiple of 32, at
+ *              most 1024), the CTA layout's and the persistent batch's calls;
+ *   CTA_GRAD   the block's gradient-only form (adjoint only);
+ *   QUADRATIC  Gaussian with symmetric C (adjoint only, width >= dim): the
+ *              CTA line search's carried point x_i + alpha p_i, from one
+ *              pass over C at (x_i, p_i) (d_p: n*dim directions): d_f =
+ *              f(x) + alpha grad f(x).p + alpha^2 f(p), d_g = C x + alpha C p.
+ * Workspace: zeus_gradient_workspace_size() bytes (the NLL's per-bin
+ * constants; 0 otherwise). */
+#define ZEUS_GRADPATH_THREAD 0
+#define ZEUS_GRADPATH_TILE 1
+#define ZEUS_GRADPATH_TILE_GRAD 2
+#define ZEUS_GRADPATH_CTA 3
+#define ZEUS_GRADPATH_CTA_GRAD 4
+#define ZEUS_GRADPATH_QUADRATIC 5
+size_t zeus_gradient_workspace_size(const zeus_problem* problem);
+int zeus_gradient_device(const zeus_problem* problem, int32_t path,
+                         int32_t gradient, int32_t width, const double* d_x,
+                         const double* d_p, double alpha, int64_t n,
+                         double* d_f, double* d_g, void* d_workspace,
+                         size_t workspace_bytes, void* stream);
+/* Bit k set: the tile layout is built with 2^k lanes per run for
+ * (kind, dim); 0 if it has no tile layout. */
+uint32_t zeus_tile_widths(int32_t kind, int32_t dim);
+
 /* ---- reduction ------------------------------------------------------
  * Replaces bfgs::launchReduction + util::dumpDataToFile's census
  * (bfgs_common.cuh:280-319, util.hpp:151-200): argmin of fval (lowest index

@@ -232,13 +232,66 @@ zref_value_grad(int kind, int dim, const double* x, double* grad)
     return f(xa);                                                              \
   }
   ZREF_VG(ZREF_ROSENBROCK, 2, util::Rosenbrock<2>)
+  ZREF_VG(ZREF_ROSENBROCK, 4, util::Rosenbrock<4>)
   ZREF_VG(ZREF_ROSENBROCK, 8, util::Rosenbrock<8>)
+  ZREF_VG(ZREF_ROSENBROCK, 10, util::Rosenbrock<10>)
+  ZREF_VG(ZREF_ROSENBROCK, 16, util::Rosenbrock<16>)
   ZREF_VG(ZREF_ROSENBROCK, 32, util::Rosenbrock<32>)
+  ZREF_VG(ZREF_ROSENBROCK, 64, util::Rosenbrock<64>)
+  ZREF_VG(ZREF_ROSENBROCK, 128, util::Rosenbrock<128>)
+  ZREF_VG(ZREF_ROSENBROCK, 256, util::Rosenbrock<256>)
   ZREF_VG(ZREF_RASTRIGIN, 2, util::Rastrigin<2>)
   ZREF_VG(ZREF_RASTRIGIN, 10, util::Rastrigin<10>)
+  ZREF_VG(ZREF_RASTRIGIN, 16, util::Rastrigin<16>)
   ZREF_VG(ZREF_ACKLEY, 2, util::Ackley<2>)
+  ZREF_VG(ZREF_ACKLEY, 10, util::Ackley<10>)
   ZREF_VG(ZREF_ACKLEY, 30, util::Ackley<30>)
 #undef ZREF_VG
+  return std::numeric_limits<double>::quiet_NaN();
+}
+
+/// zref_value_grad for the objectives that carry data: the Gaussian
+/// (examples/gaussian.hpp, C row-major dim*dim) and the Poisson NLL
+/// (simulation/fitting/LogLikelihood.h, ndata centres and counts).
+double
+zref_value_grad_data(int kind, int dim, const double* data, const int* idata,
+                     int ndata, const double* x, double* grad)
+{
+  const auto eval = [&](const auto& f, auto dimc) -> double {
+    constexpr std::size_t D = decltype(dimc)::value;
+    std::array<double, D> xa, ga;
+    for (std::size_t i = 0; i < D; ++i)
+      xa[i] = x[i];
+    dual::calculateGradientUsingAD(f, xa, ga);
+    for (std::size_t i = 0; i < D; ++i)
+      grad[i] = ga[i];
+    return f(xa);
+  };
+  const auto gaussian_vg = [&](auto dimc) -> double {
+    constexpr std::size_t D = decltype(dimc)::value;
+    auto Ch = std::make_unique<std::array<std::array<double, D>, D>>();
+    for (std::size_t i = 0; i < D; ++i)
+      for (std::size_t j = 0; j < D; ++j)
+        (*Ch)[i][j] = data[i * D + j];
+    Gaussian<D> g(*Ch);
+    return eval(g, dimc);
+  };
+  if (kind == ZREF_GAUSSIAN) {
+    if (dim == 2)
+      return gaussian_vg(std::integral_constant<std::size_t, 2>{});
+    if (dim == 8)
+      return gaussian_vg(std::integral_constant<std::size_t, 8>{});
+    if (dim == 32)
+      return gaussian_vg(std::integral_constant<std::size_t, 32>{});
+    if (dim == 150)
+      return gaussian_vg(std::integral_constant<std::size_t, 150>{});
+  }
+  if (kind == ZREF_POISSON_NLL && dim == 4) {
+    std::vector<int> counts(idata, idata + ndata);
+    std::vector<double> centres(data, data + ndata);
+    LogLikelihood ll(counts, centres);
+    return eval(ll, std::integral_constant<std::size_t, 4>{});
+  }
   return std::numeric_limits<double>::quiet_NaN();
 }
 

@@ -96,6 +96,8 @@ def ref():
         L.zref_digamma.argtypes = [C.c_double]
         L.zref_value_grad.restype = C.c_double
         L.zref_value_grad.argtypes = [C.c_int, C.c_int, _P, _P]
+        L.zref_value_grad_data.restype = C.c_double
+        L.zref_value_grad_data.argtypes = [C.c_int, C.c_int, _P, _P, C.c_int, _P, _P]
         _ref = L
     return _ref
 
@@ -209,6 +211,21 @@ def grad_dual(kind, dim, x, data=None, idata=None):
     x = np.ascontiguousarray(x, dtype=np.float64)
     g = np.zeros(dim)
     f = oracle().zor_value_grad_dual(C.byref(o), _p(x), _p(g))
+    return f, g
+
+
+def ref_grad_dual(kind, dim, x, data=None, idata=None):
+    """The reference's own dual::calculateGradientUsingAD
+    (include/duals.cuh:241-266) from its host build: (f, grad)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    g = np.zeros(dim)
+    if data is None:
+        f = ref().zref_value_grad(kind, dim, _p(x), _p(g))
+    else:
+        data = np.ascontiguousarray(data, dtype=np.float64)
+        idata = None if idata is None else np.ascontiguousarray(idata, dtype=np.int32)
+        nd = 0 if idata is None else len(idata)
+        f = ref().zref_value_grad_data(kind, dim, _p(data), _p(idata), nd, _p(x), _p(g))
     return f, g
 
 

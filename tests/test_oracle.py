@@ -309,3 +309,63 @@ def test_reference_outcomes_move_with_fma_contraction(kind, dim, lo, hi, n, iter
     print(f"kind {kind} dim {dim}: status agreement {agree:.1%}")
     assert 0.8 <= agree < 1.0
     assert np.abs(a["fval"][both] - b["fval"][both]).max() <= 1e-8
+
+
+# ---- the dual gradient pinned to the reference's own ----------------------
+def _grad_points(kind, dim, n, seed):
+    rng = np.random.default_rng(seed)
+    lo, hi = {ROS: (-5, 5), RAS: (-5.12, 5.12), ACK: (-32.768, 32.768),
+              GAU: (-5, 5)}[kind]
+    return rng.uniform(lo, hi, size=(n, dim))
+
+
+@needs_ref
+@pytest.mark.parametrize("kind,dim", [(ROS, d) for d in (2, 4, 8, 10, 16, 32, 64, 128, 256)]
+                         + [(RAS, d) for d in (2, 10, 16)] + [(ACK, d) for d in (2, 10, 30)])
+def test_oracle_dual_gradient_bit_identical_to_reference(kind, dim):
+    """zor_value_grad_dual equals the reference's dual::calculateGradientUsingAD
+    (include/duals.cuh:241-266) from its host build, bit for bit."""
+    for x in _grad_points(kind, dim, 8, 17 * dim + kind):
+        fo, go = O.grad_dual(kind, dim, x)
+        fr, gr = O.ref_grad_dual(kind, dim, x)
+        np.testing.assert_array_equal(go, gr)
+        assert fo == fr
+
+
+@needs_ref
+@pytest.mark.parametrize("dim,sym", [(2, True), (8, True), (32, True), (150, True),
+                                     (8, False), (150, False)])
+def test_oracle_dual_gradient_gaussian_bit_identical_to_reference(dim, sym):
+    rng = np.random.default_rng(dim)
+    C = np.full((dim, dim), 0.5)
+    np.fill_diagonal(C, 1.0 + (dim - 1) * 0.5)
+    if not sym:
+        C = C + 0.25 * rng.normal(size=(dim, dim))
+    C = np.ascontiguousarray(C)
+    for x in _grad_points(GAU, dim, 4, dim + 1):
+        fo, go = O.grad_dual(GAU, dim, x, C)
+        fr, gr = O.ref_grad_dual(GAU, dim, x, C)
+        np.testing.assert_array_equal(go, gr)
+        assert fo == fr
+
+
+@needs_ref
+def test_oracle_dual_gradient_nll_bit_identical_to_reference():
+    x, k, _ = O.dijet_toy()
+    rng = np.random.default_rng(11)
+    base = np.array([1.0, 10.0, 5.0, 0.1])
+    shape = (1 - x) ** base[1] / x ** (base[2] + base[3] * np.log(x))
+    base[0] = k.sum() / shape.sum()
+    for th in base * (1.0 + 0.05 * rng.normal(size=(6, 4))):
+        fo, go = O.grad_dual(NLL, 4, th, x, k)
+        fr, gr = O.ref_grad_dual(NLL, 4, th, x, k)
+        np.testing.assert_array_equal(go, gr)
+        assert fo == fr
+
+
+@needs_ref
+def test_reference_ackley_gradient_near_origin():
+    """test/fun_tests.cu:75-128 through the reference build and the oracle."""
+    for fn in (O.grad_dual, O.ref_grad_dual):
+        _, g = fn(ACK, 2, np.array([-1e-17, 1e-17]))
+        np.testing.assert_allclose(g, [-2.0, 2.0], rtol=1e-12)

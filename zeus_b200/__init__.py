@@ -34,6 +34,8 @@ MODE_EXACT, MODE_FAST = 0, 1
 GRAD_DUAL, GRAD_ADJOINT = 0, 1
 LAYOUT_AUTO, LAYOUT_THREAD, LAYOUT_TILE, LAYOUT_CTA = 0, 1, 2, 3
 FLAG_NO_FIXED_POINT = 1
+(GRADPATH_THREAD, GRADPATH_TILE, GRADPATH_TILE_GRAD, GRADPATH_CTA, GRADPATH_CTA_GRAD,
+ GRADPATH_QUADRATIC) = range(6)
 PRNG_XORWOW, PRNG_PHILOX, PRNG_SOBOL = 0, 1, 2
 
 
@@ -186,6 +188,12 @@ SIGNATURES = {
         [C.POINTER(Problem), C.POINTER(BfgsConfig), _P, C.c_int64,
          C.POINTER(RunOutputs), _P, _P, C.c_size_t, _P],
     ),
+    "zeus_gradient_workspace_size": (C.c_size_t, [C.POINTER(Problem)]),
+    "zeus_gradient_device": (
+        C.c_int,
+        [C.POINTER(Problem), C.c_int32, C.c_int32, C.c_int32, _P, _P, C.c_double,
+         C.c_int64, _P, _P, _P, C.c_size_t, _P]),
+    "zeus_tile_widths": (C.c_uint32, [C.c_int32, C.c_int32]),
     "zeus_census_device": (
         C.c_int, [_P, _P, _P, C.c_int64, C.c_int32, _P, _P, _P]),
     "zeus_optimize": (

@@ -46,6 +46,7 @@ UNITS = [
     ("zb_batch_384.cu", []),
     ("zb_noalloc.cu", ["-fmad=false"]),
     ("zb_fit.cu", []),
+    ("zb_grad.cu", []),
     ("zb_traj.cu", []),
     ("zb_sobol.cu", []),
     ("zb_runtime.cu", []),

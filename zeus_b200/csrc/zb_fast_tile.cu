@@ -5,27 +5,6 @@
 namespace zb {
 
   namespace {
-    // widths built for an objective and dimension: H rows per lane R*D <=
-    // 64 doubles; up to 4*D lanes (the spare lanes evaluate line-search
-    // trials in parallel), any width where the cooperative evaluation
-    // splits something other than the coordinates (the NLL's bins, the
-    // Gaussian's C x)
-    constexpr unsigned
-    widths_for(int kind, int d)
-    {
-      unsigned m = 0;
-      if (d > 32)
-        return 0;
-      const bool wide = kind == ZEUS_OBJ_POISSON_NLL || kind == ZEUS_OBJ_GAUSSIAN;
-      for (int k = 1; k <= 5; ++k) {
-        const int ts = 1 << k;
-        const int r = (d + ts - 1) / ts;
-        if (r * d <= 64 && (wide || ts <= 4 * d))
-          m |= 1u << k;
-      }
-      return m;
-    }
-
     template <class F, int D, int TS>
     int
     launch_ts(const F& f, bool adjoint, const BfgsParams& prm,
@@ -48,7 +27,7 @@ namespace zb {
   unsigned
   tile_widths(int kind, int dim)
   {
-    return builtin_supported(kind, dim) ? widths_for(kind, dim) : 0u;
+    return builtin_supported(kind, dim) ? tile_widths_for(kind, dim) : 0u;
   }
 
   int
@@ -60,7 +39,7 @@ namespace zb {
     return visit_objective(o, [&](auto f) -> int {
       using F = decltype(f);
       constexpr int D = (int)F::arity;
-      constexpr unsigned W = widths_for(F::kind, D);
+      constexpr unsigned W = tile_widths_for(F::kind, D);
       switch (tile) {
 #define ZB_TS(K)                                                               \
   case (1 << K):                                                               \

@@ -44,6 +44,27 @@ namespace zb {
                  size_t ws_bytes, cudaStream_t st,
                  const uint32_t* sobol = nullptr);
 
+  // Tile widths built for an objective and dimension (bit k: width 2^k):
+  // H rows per lane R*D <= 64 doubles; up to 4*D lanes (the spare lanes
+  // evaluate line-search trials in parallel), any width where the
+  // cooperative evaluation splits something other than the coordinates (the
+  // NLL's bins, the Gaussian's C x).
+  constexpr unsigned
+  tile_widths_for(int kind, int d)
+  {
+    unsigned m = 0;
+    if (d > 32)
+      return 0;
+    const bool wide = kind == ZEUS_OBJ_POISSON_NLL || kind == ZEUS_OBJ_GAUSSIAN;
+    for (int k = 1; k <= 5; ++k) {
+      const int ts = 1 << k;
+      const int r = (d + ts - 1) / ts;
+      if (r * d <= 64 && (wide || ts <= 4 * d))
+        m |= 1u << k;
+    }
+    return m;
+  }
+
   // fast-mode layouts (zb_fast_thread.cu, zb_fast_tile.cu, zb_fast_cta.cu)
   bool thread_layout_supported(int kind, int dim);
   int launch_thread(const Objective& o, const zeus_bfgs_config& c,
@@ -73,6 +94,11 @@ namespace zb {
                   const BfgsParams& prm, const double* starts,
                   const RunOut& out, Control* ctl, void* ws, size_t ws_bytes,
                   cudaStream_t st);
+
+  // gradient evaluation at given points (zb_grad.cu): path ZEUS_GRADPATH_*
+  int launch_gradient(const Objective& o, int path, int gradient, int width,
+                      const double* x, const double* p, double alpha,
+                      int64_t n, double* fo, double* go, cudaStream_t st);
 
   inline size_t
   align_up(size_t v, size_t a = 256)

@@ -536,6 +536,72 @@ zeus_bfgs_device(const zeus_problem* problem, const zeus_bfgs_config* config,
   return launch_fast(o, *config, prm, d_starts, ro, ctl, ws, kws, st);
 }
 
+size_t
+zeus_gradient_workspace_size(const zeus_problem* problem)
+{
+  if (check_problem(problem))
+    return 0;
+  return nll_bytes(problem);
+}
+
+uint32_t
+zeus_tile_widths(int32_t kind, int32_t dim)
+{
+  return tile_widths(kind, dim);
+}
+
+int
+zeus_gradient_device(const zeus_problem* problem, int32_t path,
+                     int32_t gradient, int32_t width, const double* d_x,
+                     const double* d_p, double alpha, int64_t n, double* d_f,
+                     double* d_g, void* d_workspace, size_t workspace_bytes,
+                     void* stream)
+{
+  int rc = check_problem(problem);
+  if (rc)
+    return rc;
+  if (gradient != ZEUS_GRAD_DUAL && gradient != ZEUS_GRAD_ADJOINT) {
+    set_error("unknown gradient %d", gradient);
+    return ZEUS_E_INVALID;
+  }
+  if (n < 0 || n > 0x7fffffffLL || (n > 0 && (!d_x || !d_f || !d_g))) {
+    set_error("zeus_gradient_device: bad arguments");
+    return ZEUS_E_INVALID;
+  }
+  if (path == ZEUS_GRADPATH_CTA || path == ZEUS_GRADPATH_CTA_GRAD ||
+      path == ZEUS_GRADPATH_QUADRATIC) {
+    if (width < 32 || width > 1024 || width % 32 != 0) {
+      set_error("block gradient paths: width %d is not a multiple of 32 in "
+                "[32, 1024]",
+                width);
+      return ZEUS_E_INVALID;
+    }
+    if (path == ZEUS_GRADPATH_QUADRATIC && (width < problem->dim || !d_p)) {
+      set_error("quadratic gradient path: needs width >= dim and directions");
+      return ZEUS_E_INVALID;
+    }
+  }
+  if (n == 0)
+    return ZEUS_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const double* bins = nullptr;
+  if (problem->kind == ZEUS_OBJ_POISSON_NLL) {
+    if (!d_workspace || workspace_bytes < nll_bytes(problem)) {
+      set_error("zeus_gradient_device: workspace of %zu bytes needed, got %zu",
+                nll_bytes(problem), workspace_bytes);
+      return ZEUS_E_WORKSPACE;
+    }
+    double* b = static_cast<double*>(d_workspace);
+    nll_bins_kernel<<<(problem->ndata + 127) / 128, 128, 0, st>>>(
+      problem->data, problem->idata, problem->ndata, b);
+    if ((rc = cuda_fail(cudaGetLastError(), "NLL bins launch")))
+      return rc;
+    bins = b;
+  }
+  return launch_gradient(to_objective(problem, bins), path, gradient, width,
+                         d_x, d_p, alpha, n, d_f, d_g, st);
+}
+
 int
 zeus_census_device(const double* d_fval, const int32_t* d_status,
                    const double* d_x, int64_t n, int32_t dim,

@@ -12,7 +12,7 @@ import numpy as np
 import torch
 
 from . import (BatchClass, BfgsConfig, Objective, RunOutputs, check, lib, make_config,
-               prng_code, LAYOUT_AUTO, PRNG_PHILOX)
+               prng_code, LAYOUT_AUTO, PRNG_PHILOX, GRADPATH_QUADRATIC, _GRADS)
 
 
 def _stream_handle(stream: Optional[torch.cuda.Stream]) -> int:
@@ -140,6 +140,40 @@ def bfgs_device(obj, starts: torch.Tensor, max_iter: int = 10000,
     cfg = make_config(max_iter, required, tol, mode, gradient, layout, tile, block, flags)
     r = BfgsRun(obj, n, cfg, device=starts.device, traj=traj)
     return r.launch(starts, stream=stream)
+
+
+def gradient_device(obj, x: torch.Tensor, path: int, gradient: str = "adjoint",
+                    width: int = 0, p: Optional[torch.Tensor] = None, alpha: float = 0.0,
+                    stream=None):
+    """f and grad f at the rows of ``x`` (n, dim) through one gradient path of
+    the BFGS layouts (GRADPATH_*: thread, tile / tile gradient-only of
+    ``width`` lanes, CTA / CTA gradient-only of ``width`` threads, or the
+    quadratic form's carried point x + alpha p).  Returns (f (n,), g (n, dim))."""
+    dp = _as_problem(obj, x.device)
+    dim = dp.obj.dim
+    if x.dtype != torch.float64 or not x.is_cuda or x.dim() != 2 or x.shape[1] != dim:
+        raise ValueError(f"x must be a float64 CUDA tensor of shape (n, {dim})")
+    x = x.contiguous()
+    if path == GRADPATH_QUADRATIC:
+        if p is None or p.shape != x.shape:
+            raise ValueError("the quadratic path needs directions p shaped like x")
+        p = p.contiguous()
+    n = x.shape[0]
+    fo = torch.empty((n,), dtype=torch.float64, device=x.device)
+    go = torch.empty((n, dim), dtype=torch.float64, device=x.device)
+    prob = dp.c()
+    wsz = lib().zeus_gradient_workspace_size(C.byref(prob))
+    ws = torch.empty((max(wsz, 1),), dtype=torch.uint8, device=x.device)
+    check(lib().zeus_gradient_device(C.byref(prob), path, _GRADS[gradient], width, _ptr(x),
+                                     _ptr(p), alpha, n, _ptr(fo), _ptr(go), _ptr(ws), wsz,
+                                     _stream_handle(stream)))
+    return fo, go
+
+
+def tile_widths(kind: int, dim: int) -> list[int]:
+    """Lanes per run the tile layout is built with for (kind, dim)."""
+    m = lib().zeus_tile_widths(kind, dim)
+    return [1 << k for k in range(1, 6) if (m >> k) & 1]
 
 
 def census_device(fval: torch.Tensor, status: torch.Tensor, x: Optional[torch.Tensor],
