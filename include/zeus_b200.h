@@ -332,7 +332,7 @@ int zeus_autotune_record(int32_t kind, int32_t dim, int32_t gradient,
  *   TILE_GRAD  the tile's gradient-only form (adjoint only; f from the
  *              cooperative value) -- the form tile_run calls;
  *   CTA        a block of `width` threads per point (a multiple of 32, at
- *              most 1024), the CTA layout's and the persistent batch's calls;
+ *              most 512), the CTA layout's and the persistent batch's calls;
  *   CTA_GRAD   the block's gradient-only form (adjoint only);
  *   QUADRATIC  Gaussian with symmetric C (adjoint only, width >= dim): the
  *              CTA line search's carried point x_i + alpha p_i, from one

@@ -119,5 +119,79 @@ def build_dropin_test(verbose: bool = False) -> Path:
     return DROPIN_BIN
 
 
+REF_EXAMPLES_BIN = BIN / "ref_examples"
+# programs built from the reference's examples, unchanged, against include/:
+# name -> (sources relative to the reference's examples/ directory, or to
+# this repository for the repo's own driver)
+REF_PROGRAMS = {
+    "optimize_rosenbrock": ["optimize_rosenbrock.cu", "optimization_utils.cc"],
+    "optimize_rastrigin": ["optimize_rastrigin.cu", "optimization_utils.cc"],
+    "optimize_ackley": ["optimize_ackley.cu", "optimization_utils.cc"],
+    "fit_dijet_spectrum": ["fit_dijet_spectrum.cu"],
+    "ref_objectives_test": [ROOT / "tests" / "cpp" / "ref_objectives_test.cu"],
+}
+
+
+def _ref_tree(reference_dir: Path) -> Path:
+    """A build tree in which the reference's example sources sit beside this
+    library's include/ in place of the reference's own:
+    <tree>/examples/<file> are links to the reference's example files, and
+    <tree>/include links to include/, so a relative include such as
+    "../include/traits.hpp" (optimization_utils.hpp:4) reaches this
+    library's header.  Only links are made; no source is copied."""
+    tree = BUILD / "ref_examples"
+    ex = tree / "examples"
+    (ex / "simulation" / "fitting").mkdir(parents=True, exist_ok=True)
+    src = Path(reference_dir) / "examples"
+    files = [f for f in src.iterdir() if f.is_file()]
+    files.append(src / "simulation" / "fitting" / "LogLikelihood.h")
+    for f in files:
+        link = ex / f.relative_to(src)
+        if link.is_symlink() and link.resolve() == f.resolve():
+            continue
+        if link.is_symlink() or link.exists():
+            link.unlink()
+        link.symlink_to(f)
+    inc = tree / "include"
+    if not inc.is_symlink():
+        inc.symlink_to(INCLUDE)
+    return tree
+
+
+def build_reference_examples(reference_dir, verbose: bool = False) -> list[Path]:
+    """Compiles the reference's example programs (optimize_rosenbrock.cu,
+    optimize_rastrigin.cu, optimize_ackley.cu with optimization_utils.cc,
+    fit_dijet_spectrum.cu) and tests/cpp/ref_objectives_test.cu (which
+    includes the reference's gaussian.hpp and LogLikelihood.h) against this
+    library's include/ and libzeus_b200.so, into zeus_b200/_bin/ref_examples/.
+    The reference's sources are compiled where they lie, unmodified."""
+    lib = build(verbose)
+    tree = _ref_tree(Path(reference_dir))
+    REF_EXAMPLES_BIN.mkdir(parents=True, exist_ok=True)
+    headers = [INCLUDE / h for h in ("zeus.cuh", "duals.cuh", "matrix.hpp", "traits.hpp")]
+    deps_common = headers + [lib] + list(CSRC.glob("*.cuh"))
+
+    def one(item):
+        name, srcs = item
+        paths = [s if isinstance(s, Path) else tree / "examples" / s for s in srcs]
+        out = REF_EXAMPLES_BIN / name
+        newest = max(p.stat().st_mtime for p in deps_common + [q.resolve() for q in paths])
+        if out.exists() and out.stat().st_mtime >= newest:
+            return out
+        cmd = [nvcc(), *COMMON, "-I", str(tree / "examples"), *map(str, paths), "-o",
+               str(out), "-L", str(HERE), "-lzeus_b200", "-Xlinker",
+               "-rpath,$ORIGIN/../.."]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"{name}: build against include/ failed:\n{r.stdout}\n"
+                               f"{r.stderr}")
+        return out
+
+    with cf.ThreadPoolExecutor(max_workers=len(REF_PROGRAMS)) as ex:
+        return list(ex.map(one, REF_PROGRAMS.items()))
+
+
 if __name__ == "__main__":
     print(build(verbose="-v" in sys.argv))

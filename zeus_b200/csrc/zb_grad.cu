@@ -106,8 +106,11 @@ namespace zb {
       return 2 * de + kCtaRedDoubles + (size_t)block;
     }
 
+    // blocks of up to 512 threads, the widest the BFGS kernels launch
+    constexpr int kGradMaxBlock = 512;
+
     template <class F, int D, bool Adjoint, bool GradOnly>
-    __global__ void
+    __global__ void __launch_bounds__(kGradMaxBlock)
     grad_cta_kernel(F f, const double* __restrict__ x, double* __restrict__ fo,
                     double* __restrict__ go)
     {
@@ -159,7 +162,7 @@ namespace zb {
     }
 
     template <class F, int D>
-    __global__ void
+    __global__ void __launch_bounds__(kGradMaxBlock)
     grad_quad_kernel(F f, const double* __restrict__ x,
                      const double* __restrict__ p, double alpha,
                      double* __restrict__ fo, double* __restrict__ go)

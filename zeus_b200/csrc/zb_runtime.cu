@@ -570,9 +570,9 @@ zeus_gradient_device(const zeus_problem* problem, int32_t path,
   }
   if (path == ZEUS_GRADPATH_CTA || path == ZEUS_GRADPATH_CTA_GRAD ||
       path == ZEUS_GRADPATH_QUADRATIC) {
-    if (width < 32 || width > 1024 || width % 32 != 0) {
+    if (width < 32 || width > 512 || width % 32 != 0) {
       set_error("block gradient paths: width %d is not a multiple of 32 in "
-                "[32, 1024]",
+                "[32, 512]",
                 width);
       return ZEUS_E_INVALID;
     }
