@@ -6,8 +6,10 @@ A step is one full optimisation call on the workload: PSO seeding (or
 uniform starts when the workload has PSO off), every BFGS run, and the
 argmin/census reduction, with inputs resident in HBM.  `value` counts the
 runs that finish with status 1 (||grad|| < tol) per second of device time;
-`e2e` is the same metric through the host-buffer C-ABI call zeus_optimize
-(host inputs in, host result out, copies inside the timed region).
+`e2e` is the same metric through the public host-buffer calls -- the batch
+plan zeus_batch_plan_run for batched workloads, zeus_optimize otherwise --
+with the host inputs (starts, objective data) copied in and every class's
+best run, coordinates and census copied back inside the timed region.
 
   python bench.py [--workload W] [--steps K] [--warmup W] [--gpus N]
   python bench.py --impl reference ...   # the reference's own sequential
@@ -145,11 +147,15 @@ class Job:
     in a persistent batch."""
 
     def __init__(self, name, obj_fn, n, lo, hi, pso_iter, max_iter, required, tol=1e-8,
-                 runs_per_instance=0):
+                 runs_per_instance=0, ref_runs=8):
         self.name, self.obj_fn, self.n = name, obj_fn, n
         self.lo, self.hi, self.pso_iter = lo, hi, pso_iter
         self.max_iter, self.required, self.tol = max_iter, required, tol
         self.runs_per_instance = runs_per_instance
+        # whole runs of this class in each step of the reference's timed
+        # sample (0: the class is too heavy for the reference to finish a
+        # run inside a step; it enters only the whole-workload estimate)
+        self.ref_runs = ref_runs
         self.n_full = n  # before --scale: the objective's data holds n_full / rpi instances
 
     def make_objective(self):
@@ -193,10 +199,13 @@ def workloads():
                  "(Philox, seed 42 + class), PSO off, <=10000 iters, tol 1e-8, "
                  "stop-early off",
             batch=True,
+            # the reference's O(D^4) update: ~0.2 s per 128-D iteration and
+            # ~12 ms per 64-D iteration on one host core, minutes to half an
+            # hour per run, so those two classes are estimated, not sampled
             jobs=[Job("rosenbrock128", lambda: zb.Rosenbrock(128), 1365, -5.0, 5.0, -1,
-                      10000, 1 << 30),
+                      10000, 1 << 30, ref_runs=0),
                   Job("rosenbrock64", lambda: zb.Rosenbrock(64), 1365, -5.0, 5.0, -1,
-                      10000, 1 << 30),
+                      10000, 1 << 30, ref_runs=0),
                   Job("ackley30", lambda: zb.Ackley(30), 1365, -32.768, 32.768, -1,
                       10000, 1 << 30),
                   Job("rosenbrock32", lambda: zb.Rosenbrock(32), 1365, -5.0, 5.0, -1,
@@ -210,7 +219,7 @@ def workloads():
                  "PSO 10, <=10000 iters, tol 1e-8, stop-early off",
             batch=False,
             jobs=[Job("gaussian150", lambda: zb.Gaussian(zb.gaussian_matrix(150)), 1024,
-                      -5.0, 5.0, 10, 10000, 1 << 30)]),
+                      -5.0, 5.0, 10, 10000, 1 << 30, ref_runs=16)]),
         "multimodal": dict(
             desc="Rastrigin-10 (A=10) 16384 starts in +-5.12 and Ackley-30 16384 starts "
                  "in +-32.768, PSO 20 each (CUDA graph), <=10000 iters, tol 1e-8, "
@@ -235,6 +244,17 @@ def workloads():
             jobs=[Job("rosenbrock2", lambda: zb.Rosenbrock(2), 1024, -5.0, 5.0, 10,
                       10000, 100)]),
     }
+
+
+METRIC = "converged runs/s at ||grad||<1e-8"
+
+
+def workload_config(args, wl, world):
+    """The workload the metric is quoted on; the same dict in both arms."""
+    return {"workload": args.workload, "description": wl["desc"],
+            "runs_per_step": sum(j.n for j in wl["jobs"]) * world,
+            "l2": "1 GiB buffer written between timed steps (GPU arm)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
 
 
 # ---------------------------------------------------------------- clocks
@@ -471,18 +491,6 @@ def run_gpu(args, rank, world, local_rank):
         clocks.stop()
     counters = [((s["obj"].kind, s["obj"].dim, "adjoint", max(s["nbins"], 100)),
                  o.counters.cpu().numpy()) for s, o in zip(state, outs)]
-    iters_per_class = [o.iter.cpu().numpy() for o in outs]
-    status_per_class = [o.status.cpu().numpy() for o in outs]
-    if args.write_iterations and rank == 0:
-        path = Path(args.write_iterations)
-        doc = json.loads(path.read_text()) if path.exists() else {}
-        doc[args.workload] = {
-            s["job"].name: {"mean_iterations": float(np.mean(it)),
-                            "converged_fraction": float(np.mean(st == 1)),
-                            "runs": int(len(it))}
-            for s, it, st in zip(state, iters_per_class, status_per_class)}
-        path.write_text(json.dumps(doc, indent=1, sort_keys=True) + "\n")
-
     step_ms = float(np.mean(times))
     conv_mean = float(np.mean(conv))
     conv_all, step_ms_all = job_totals(conv_mean, step_ms, world, dev)
@@ -538,60 +546,89 @@ def run_gpu(args, rank, world, local_rank):
                              "default layout by dimension",
                      "speedup_of_headline": value / pv if pv > 0 else None}
 
-    # e2e: pinned host inputs -> device, the same step, D2H of the census
+    # e2e: through the public host-buffer calls -- a batch plan
+    # (zeus_batch_plan_run: host starts and objective data in, every class's
+    # best run, coordinates and census out, one synchronisation) for batched
+    # workloads, zeus_optimize (the zeus::Zeus of one objective) otherwise --
+    # with the host inputs in pinned memory and every copy inside the timed
+    # region
     e2e_ms, e2e_conv = [], []
-    host_inputs = []
-    for s in state:
-        hi = {}
-        if s["job"].pso_iter < 0:
-            hi["starts"] = s["starts"].cpu().pin_memory()
-        if s["dp"].data is not None:
-            hi["data"] = s["dp"].data.cpu().pin_memory()
-        if s["dp"].idata is not None:
-            hi["idata"] = s["dp"].idata.cpu().pin_memory()
-        host_inputs.append(hi)
-    h2d = sum(t.numel() * t.element_size() for hi in host_inputs for t in hi.values())
-    cen_host = torch.zeros((len(state), 6), dtype=torch.int32).pin_memory()
-    d2h = cen_host.numel() * 4
-    for k in range(args.warmup + args.steps):
-        torch.cuda.synchronize()
-        t_a = time.perf_counter()
-        for s, hi in zip(state, host_inputs):
-            if "starts" in hi:
-                s["starts"].copy_(hi["starts"], non_blocking=True)
-            if "data" in hi:
-                s["dp"].data.copy_(hi["data"], non_blocking=True)
-            if "idata" in hi:
-                s["dp"].idata.copy_(hi["idata"], non_blocking=True)
+    h2d = d2h = 0
+    e2e_api = None
+    if batch is not None:
+        specs = []
         for s in state:
-            if s["job"].pso_iter >= 0:
-                gen_starts(s)
-        if batch is not None:
-            batch.launch(stream)
-            o2 = [s["bj"] for s in state]
-        else:
-            for s in state:
-                s["run"].launch(s["starts"], stream=stream)
-            o2 = [s["run"] for s in state]
-        for i, (s, o) in enumerate(zip(state, o2)):
-            census(s, o)
-            cen_host[i].copy_(s["cen"], non_blocking=True)
-        stream.synchronize()
-        t_b = time.perf_counter()
-        if k >= args.warmup:
-            e2e_ms.append((t_b - t_a) * 1e3)
-            e2e_conv.append(int(cen_host[:, 1].sum()))
+            j, obj = s["job"], s["obj"]
+            hobj = zb.Objective(obj.kind, obj.dim, name=obj.name)
+            if s["dp"].data is not None:
+                hobj.data = s["dp"].data.cpu().pin_memory().numpy()
+            if s["dp"].idata is not None:
+                hobj.idata = s["dp"].idata.cpu().pin_memory().numpy()
+            spec = dict(obj=hobj, n=j.n, runs_per_instance=j.runs_per_instance,
+                        required=j.required)
+            if j.pso_iter < 0:
+                spec["starts"] = s["starts"].cpu().pin_memory().numpy()
+            else:
+                spec.update(seed=s["seed"], lower=j.lo, upper=j.hi, pso_iter=j.pso_iter)
+            specs.append(spec)
+        plan = zb.BatchPlan(specs, jobs[0].max_iter, jobs[0].tol)
+        e2e_api = "zeus_batch_plan_run"
+        for k in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            t_a = time.perf_counter()
+            res = plan.run(stream=stream)
+            t_b = time.perf_counter()
+            if k >= args.warmup:
+                e2e_ms.append((t_b - t_a) * 1e3)
+                e2e_conv.append(sum(r.c.claimed for r in res))
+        h2d, d2h = plan.traffic()
+        plan.close()
+    else:
+        e2e_api = "zeus_optimize"
+        hprobs = []
+        for s in state:
+            obj = s["obj"]
+            hobj = zb.Objective(obj.kind, obj.dim, name=obj.name)
+            if s["dp"].data is not None:
+                hobj.data = s["dp"].data.cpu().pin_memory().numpy()
+            if s["dp"].idata is not None:
+                hobj.idata = s["dp"].idata.cpu().pin_memory().numpy()
+            hprobs.append(hobj)
+        for k in range(args.warmup + args.steps):
+            torch.cuda.synchronize()
+            t_a = time.perf_counter()
+            conv_k = 0
+            for s, hobj in zip(state, hprobs):
+                j = s["job"]
+                cfg = zb.make_config(j.max_iter, j.required, j.tol, "fast", "adjoint")
+                best, cen = zb.CResult(), zb.CCensus()
+                bx = np.zeros(hobj.dim)
+                prob = hobj.host_problem()
+                zb.check(L.zeus_optimize(C.byref(prob), j.lo, j.hi, j.n, j.max_iter,
+                                         j.pso_iter, j.required, j.tol, s["seed"],
+                                         C.byref(cfg), C.byref(best), bx.ctypes.data,
+                                         C.byref(cen), None, None, sh))
+                conv_k += cen.claimed
+            t_b = time.perf_counter()
+            if k >= args.warmup:
+                e2e_ms.append((t_b - t_a) * 1e3)
+                e2e_conv.append(conv_k)
+        h2d = sum(0 if h.data is None else h.data.nbytes + (0 if h.idata is None
+                                                              else h.idata.nbytes)
+                  for h in hprobs)
+        d2h = len(state) * (C.sizeof(zb.CResult) + C.sizeof(zb.CCensus)) + \
+            sum(8 * h.dim for h in hprobs)
     e2e_units, e2e_ms_all = job_totals(float(np.mean(e2e_conv)), float(np.mean(e2e_ms)),
                                        world, dev)
     e2e_val = e2e_units / (e2e_ms_all * 1e-3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args, state, iters_per_class, status_per_class)
+        cpu = cpu_baseline(args)
 
     if rank == 0:
         line = {
-            "metric": "converged runs/s at ||grad||<1e-8 (adjoint+persistent-batched form)",
+            "metric": METRIC,
             "value": value,
             "unit": "runs/s",
             "n_gpus": world,
@@ -603,13 +640,10 @@ def run_gpu(args, rank, world, local_rank):
             "vs_baseline": None,
             "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": args.workload, "description": wl["desc"],
-                       "gradient": "adjoint", "mode": "fast",
-                       "batched": bool(wl["batch"]), "autotuned_layouts": tuned,
-                       "converged_per_step": conv_all,
-                       "runs_per_step": sum(j.n for j in jobs) * world,
-                       "l2": "1 GiB buffer written between timed steps",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "config": workload_config(args, wl, world),
+            "form": {"gradient": "adjoint", "mode": "fast", "batched": bool(wl["batch"]),
+                     "autotuned_layouts": tuned},
+            "converged_per_step": conv_all,
             "plain_dual": plain,
             "roofline": {"bound": "fp64", "kernel": "bfgs_batch_kernel" if batch is not None
                          else "bfgs (standalone launches)",
@@ -620,7 +654,8 @@ def run_gpu(args, rank, world, local_rank):
                          "flops_per_step": flops, "kernel_ms": kms,
                          **traffic_of(args.workload)},
             "e2e": {"value": e2e_val, "unit": "runs/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms_all},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms_all,
+                    "api": e2e_api},
             "gpu_launches": launches,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
@@ -654,131 +689,198 @@ def _ref_lib():
     return O, None
 
 
-ITERS_FIXTURE = ROOT / "tests" / "golden" / "workload_iterations.json"
-# per class: runs of the reference's sequential BFGS timed to completion,
-# or (heavy classes, where one run can take minutes) iterations per run
-# timed on one run per core and scaled by the workload's iteration counts
-FULL_SAMPLE = {2: 1024, 4: 256, 8: 128, 10: 128, 16: 64, 30: 16, 32: 16}
-ITER_SAMPLE = {64: 20, 128: 4, 150: 5}
+PARITY_FIXTURE = ROOT / "tests" / "golden" / "parity_mixed.npz"
 
 
-def _class_sample(O, obj, job, starts_host, cores, iters=None, statuses=None):
-    """Estimated (converged runs, core-seconds) of the whole class on the
-    reference host build, and a description of the sample."""
-    d = obj.dim
-    n = job.n
+def _class_data(obj, job):
+    """The objective data of the class's first instance (the runs sampled
+    from a per-instance class all use that instance)."""
     data, idata = obj.data, obj.idata
-    if job.runs_per_instance:  # one data instance (the first toy)
-        nb = len(obj.idata) // ((n + job.runs_per_instance - 1) // job.runs_per_instance)
-        data, idata = obj.data[:nb], obj.idata[:nb]
-    if d in ITER_SAMPLE:
-        m = ITER_SAMPLE[d]
-        k = min(cores, n)
-        with _QuietStdout():
-            t0 = time.perf_counter()
-            O.ref_bfgs(obj.kind, d, starts_host[:k], max_iter=m, required=1 << 30,
-                       tol=job.tol, data=data, idata=idata, lower=job.lo, upper=job.hi,
-                       nthreads=cores)
-            wall = time.perf_counter() - t0
-        t_iter = wall / m  # seconds per iteration on one core (k runs in parallel)
-        if iters is None:
-            return None, None, "no iteration counts"
-        core_s = float(np.sum(np.maximum(iters, 1))) * t_iter
-        conv = float((statuses == 1).sum())
-        return conv, core_s, (f"{job.name}: {k} runs x {m} iterations timed "
-                              f"({t_iter * 1e3:.1f} ms/iteration/core), scaled by the "
-                              f"workload's {int(np.sum(iters))} iterations")
-    k = min(FULL_SAMPLE.get(d, 64), n)
+    if job.runs_per_instance and idata is not None:
+        nb = len(idata) // max(1, (job.n + job.runs_per_instance - 1) // job.runs_per_instance)
+        data, idata = data[:nb], idata[:nb]
+    return data, idata
+
+
+def _ref_classes(O, wl, seed):
+    """(job, objective, host starts) of every class of the workload: the
+    oracle's Philox starts (equal to the GPU's bit for bit) or, with PSO, the
+    oracle's synchronous PSO from the same seed."""
+    out = []
+    for ci, j in enumerate(wl["jobs"]):
+        obj = j.make_objective()
+        data, idata = _class_data(obj, j)
+        if j.pso_iter >= 0:
+            st, _, _, _ = O.oracle_pso(obj.kind, obj.dim, seed + ci, j.n, j.lo, j.hi,
+                                       j.pso_iter, data=data, idata=idata)
+        else:
+            m = j.runs_per_instance or j.n
+            st = O.oracle_starts(seed + ci, m, obj.dim, j.lo, j.hi)
+        out.append((j, obj, np.ascontiguousarray(st)))
+    return out
+
+
+def _ref_step(O, classes, k, cores):
+    """One step of the reference's timed sample: runs k*s .. k*s+s-1
+    (wrapping) of every sampled class, s = job.ref_runs, each run to
+    completion on the reference's sequential BFGS (host build), the classes
+    concurrently with the host threads split among them.  Returns
+    (converged runs, wall seconds, runs, statuses per class)."""
+    live = [c for c in classes if c[0].ref_runs > 0]
+    if not live:
+        return 0, 0.0, 0, []
+    per = max(1, cores // len(live))
+    res = [None] * len(live)
+
+    def work(ci):
+        j, obj, st = live[ci]
+        s = j.ref_runs
+        idx = (np.arange(s) + k * s) % len(st)
+        data, idata = _class_data(obj, j)
+        res[ci] = O.ref_bfgs(obj.kind, obj.dim, st[idx], max_iter=j.max_iter,
+                             required=j.required, tol=j.tol, data=data, idata=idata,
+                             lower=j.lo, upper=j.hi, nthreads=per)
+
     with _QuietStdout():
         t0 = time.perf_counter()
-        r = O.ref_bfgs(obj.kind, d, starts_host[:k], max_iter=job.max_iter,
-                       required=job.required, tol=job.tol, data=data, idata=idata,
-                       lower=job.lo, upper=job.hi, nthreads=cores)
+        th = [threading.Thread(target=work, args=(ci,)) for ci in range(len(live))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
         wall = time.perf_counter() - t0
-    conv = float((r["status"] == 1).sum()) * n / k
-    core_s = wall * cores * n / k
-    return conv, core_s, f"{job.name}: {k} of {n} runs to completion"
+    conv = int(sum((r["status"] == 1).sum() for r in res))
+    return conv, wall, int(sum(len(r["status"]) for r in res)), \
+        {j.name: r["status"] for (j, _, _), r in zip(live, res)}
 
 
-def cpu_baseline(args, state, iters_per_class, status_per_class):
-    """The reference's sequential BFGS (host build, all host threads) on a
-    bounded sample of this workload, same starts as the GPU's last step."""
+def _ref_estimate(O, classes, conv_by_class, core_s_by_class, cores, workload):
+    """Whole-workload estimate for the reference: sampled classes scaled from
+    their measured runs; unsampled (heavy) classes from a measured
+    per-iteration time (a few iterations of `cores` runs at once) times the
+    reference's own per-run iteration counts and statuses -- those of the
+    oracle, which follows the reference's arithmetic bit for bit
+    (tests/golden/parity_mixed.npz) -- scaled to the class's runs."""
+    total_conv, total_core_s, parts = 0.0, 0.0, []
+    fx = np.load(PARITY_FIXTURE) if PARITY_FIXTURE.exists() and workload == "mixed" else None
+    for j, obj, st in classes:
+        if j.ref_runs > 0:
+            runs = max(1, conv_by_class[j.name][1])
+            total_conv += conv_by_class[j.name][0] * j.n / runs
+            total_core_s += core_s_by_class[j.name] * j.n / runs
+            parts.append(f"{j.name}: sampled")
+            continue
+        if fx is None or f"{j.name}/iter" not in fx:
+            return None
+        m_it = 3
+        k = min(cores, len(st))
+        data, idata = _class_data(obj, j)
+        with _QuietStdout():
+            t0 = time.perf_counter()
+            O.ref_bfgs(obj.kind, obj.dim, st[:k], max_iter=m_it, required=1 << 30, tol=j.tol,
+                       data=data, idata=idata, lower=j.lo, upper=j.hi, nthreads=cores)
+            t_iter = (time.perf_counter() - t0) / m_it  # per iteration per core
+        it = fx[f"{j.name}/iter"].astype(np.float64)
+        stt = fx[f"{j.name}/status"]
+        scale = j.n / len(it)
+        total_core_s += float(np.maximum(it, 1).sum()) * t_iter * scale
+        total_conv += float((stt == 1).sum()) * scale
+        parts.append(f"{j.name}: {t_iter * 1e3:.1f} ms per iteration per core x the "
+                     f"reference's {int(it.sum())} iterations over {len(it)} runs, "
+                     f"scaled by {scale:.2f}")
+    wall = total_core_s / cores
+    return {"value": total_conv / wall, "unit": "runs/s",
+            "seconds_for_workload": wall, "method": "; ".join(parts)}
+
+
+def measure_reference(args, steps, warmup, cores):
+    """The reference's own sequential BFGS (host build, all host threads) on
+    a bounded sample of the workload: per step, whole runs of every sampled
+    class (the same starts as the GPU arm).  Returns the measured record and
+    the whole-workload estimate, or (None, why)."""
     O, why = _ref_lib()
     if O is None:
+        return None, why
+    wl = workloads()[args.workload]
+    classes = _ref_classes(O, wl, args.seed)
+    live = [j for j, _, _ in classes if j.ref_runs > 0]
+    if not live:
+        return None, "no class of this workload finishes a reference run inside a step"
+    for k in range(warmup):  # untimed: one run of each sampled class
+        small = [(j, o, st) for j, o, st in classes]
+        saved = [j.ref_runs for j, _, _ in small]
+        for j, _, _ in small:
+            j.ref_runs = min(j.ref_runs, 1)
+        _ref_step(O, small, k, cores)
+        for (j, _, _), r in zip(small, saved):
+            j.ref_runs = r
+    conv, wall, runs = [], [], 0
+    by_class, core_s = {j.name: [0, 0] for j in live}, {j.name: 0.0 for j in live}
+    for k in range(steps):
+        c, w, r, st = _ref_step(O, classes, k, cores)
+        conv.append(c)
+        wall.append(w)
+        runs += r
+        for name, v in st.items():
+            by_class[name][0] += int((v == 1).sum())
+            by_class[name][1] += len(v)
+            core_s[name] += w * cores / len(st)
+    value = float(np.sum(conv)) / float(np.sum(wall))
+    sample = (f"{steps} steps x whole runs of the classes " +
+              ", ".join(f"{j.name} ({j.ref_runs} runs/step)" for j in live) +
+              f", {cores} host threads; {runs} runs, {int(np.sum(conv))} converged")
+    skipped = [j.name for j, _, _ in classes if j.ref_runs == 0]
+    if skipped:
+        sample += ("; not in the timed sample (one reference run takes minutes): " +
+                   ", ".join(skipped))
+    est = _ref_estimate(O, classes, by_class, core_s, cores, args.workload)
+    return {"value": value, "ms_per_step": float(np.mean(wall)) * 1e3,
+            "converged_per_step": float(np.mean(conv)), "sample": sample,
+            "by_class": {k: {"converged": v[0], "runs": v[1]} for k, v in by_class.items()},
+            "estimate_full_workload": est}, None
+
+
+def cpu_baseline(args):
+    """The reference's sequential BFGS (host build, all host threads) on one
+    step's bounded sample of this workload, on the GPU arm's starts."""
+    cores = os.cpu_count() or 1
+    rec, why = measure_reference(args, 2, 0, cores)
+    if rec is None:
         return {"value": None, "unit": "runs/s", "cores": 0, "kind": "reference",
                 "sample": why}
-    cores = os.cpu_count() or 1
-    conv, core_s, desc = 0.0, 0.0, []
-    for s, it, st in zip(state, iters_per_class, status_per_class):
-        c, cs, dsc = _class_sample(O, s["obj"], s["job"], s["starts"].cpu().numpy(), cores,
-                                   it, st)
-        conv += c
-        core_s += cs
-        desc.append(dsc)
-    wall = core_s / cores
-    return {"value": conv / wall, "unit": "runs/s", "cores": cores, "kind": "reference",
-            "sample": "; ".join(desc), "estimated_seconds_for_workload": wall}
+    return {"value": rec["value"], "unit": "runs/s", "cores": cores, "kind": "reference",
+            "sample": rec["sample"], "estimate_full_workload": rec["estimate_full_workload"]}
 
 
 def run_reference(args, rank, world):
     """The reference's own CPU implementation of the path (its sequential BFGS
-    built for the host) on the same workload, all host threads.  Heavy
-    classes are timed per iteration and scaled by the workload's per-run
-    iteration counts recorded in tests/golden/workload_iterations.json."""
+    built for the host, oracle/_ref) on this workload: each step runs whole
+    reference runs of a rotating sample of every class that can finish a run
+    inside a step, on all host threads; `value` is their converged runs per
+    second of wall time, measured.  The whole-workload estimate (heavy
+    classes from measured per-iteration times) is reported beside it."""
     if rank != 0:
         return
-    O, why = _ref_lib()
     wl = workloads()[args.workload]
-    if O is None:
+    cores = os.cpu_count() or 1
+    rec, why = measure_reference(args, args.steps, args.warmup, cores)
+    if rec is None:
         print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
         return
-    fixture = {}
-    if ITERS_FIXTURE.exists():
-        fixture = json.loads(ITERS_FIXTURE.read_text()).get(args.workload, {})
-    cores = os.cpu_count() or 1
-    sts = []
-    for ci, j in enumerate(wl["jobs"]):
-        obj = j.obj_fn()
-        seed = args.seed + ci
-        if j.pso_iter >= 0:
-            pbx, _, _, _ = O.oracle_pso(obj.kind, obj.dim, seed, j.n, j.lo, j.hi,
-                                        j.pso_iter, data=obj.data if obj.kind == 3 else None)
-        else:
-            pbx = O.oracle_starts(seed, min(j.n, 4096), obj.dim, j.lo, j.hi)
-        sts.append((j, obj, pbx))
-    times, convs, desc = [], [], []
-    for k in range(args.warmup + args.steps):
-        conv, core_s, desc = 0.0, 0.0, []
-        for j, obj, pbx in sts:
-            fx = fixture.get(j.name)
-            it = st = None
-            if fx is not None:
-                it = np.full(j.n, fx["mean_iterations"])
-                st = np.zeros(j.n, np.int32)
-                st[:int(round(fx["converged_fraction"] * j.n))] = 1
-            c, cs, dsc = _class_sample(O, obj, j, pbx, cores, it, st)
-            if c is None:
-                print(json.dumps({"impl": "reference", "unavailable":
-                                  f"{j.name}: per-run iteration counts missing from "
-                                  f"{ITERS_FIXTURE.name}"}), flush=True)
-                return
-            conv += c
-            core_s += cs
-            desc.append(dsc)
-        if k >= args.warmup:
-            times.append(core_s / cores)
-            convs.append(conv)
-    v = float(np.mean(convs)) / float(np.mean(times))
+    v = rec["value"]
     print(json.dumps({
         "impl": "reference",
-        "metric": "converged runs/s at ||grad||<1e-8 (adjoint+persistent-batched form)",
+        "metric": METRIC,
         "value": v, "unit": "runs/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": float(np.mean(times)) * 1e3,
+        "warmup": args.warmup, "ms_per_step": rec["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "description": wl["desc"]},
+        "config": workload_config(args, wl, world),
+        "converged_per_step": rec["converged_per_step"],
+        "by_class": rec["by_class"],
+        "estimate_full_workload": rec["estimate_full_workload"],
         "cpu_baseline": {"value": v, "unit": "runs/s", "cores": cores, "kind": "reference",
-                         "sample": "; ".join(desc)},
+                         "sample": rec["sample"]},
         "e2e": {"value": v, "unit": "runs/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -801,8 +903,6 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--scale", type=float, default=1.0,
                     help="multiply every class's run count (small cases for profiling)")
-    ap.add_argument("--write-iterations", default="",
-                    help="write per-class iteration statistics (for the reference arm)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -282,6 +282,51 @@ int zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
                       const zeus_bfgs_config* config, void* d_workspace,
                       size_t workspace_bytes, void* stream);
 
+/* ---- persistent batch with host buffers --------------------------------
+ * The reference runs one objective per zeus::Zeus call, with host inputs
+ * and a host Result back (zeus.cuh:341-375; the best run by
+ * bfgs_common.cuh:280-319).  A batch plan does that for up to 16 classes in
+ * one persistent kernel launch: it owns the device copies of every class's
+ * objective data and starts, the per-run outputs and the batch workspace,
+ * allocated once at creation on the current device.  Each run copies the
+ * classes' HOST inputs to the device (objective data, and starts when given;
+ * without host starts a class draws them on the device from `seed`: PSO
+ * when pso_iter >= 0, as pso::launch, else uniform Philox starts in
+ * [lower, upper)), runs zeus_batch_device, reduces every class (argmin with
+ * ties to the lowest index, census as zeus_census_device) and returns per
+ * class the best run (best[c]), its coordinates (best_x: the classes'
+ * coordinates one after another, sum of dims doubles) and the census
+ * (census[c], may be NULL), with one device-to-host copy and one
+ * synchronisation of `stream`.  Runs must use the plan's device and class
+ * shapes (kind, dim, ndata, n, runs_per_instance, host-or-device starts);
+ * the data and starts may change between runs.  Errors set every
+ * best[c].status to 3 (allocation) or 4 (CUDA), as zeus_optimize does. */
+typedef struct zeus_host_class {
+  zeus_problem problem;       /* data / idata: HOST pointers to every instance */
+  int64_t n;                  /* runs */
+  int64_t runs_per_instance;  /* 0: every run uses the one instance */
+  const double* starts;       /* HOST n*dim starts, or NULL: drawn on the device */
+  uint64_t seed;              /* starts == NULL: the generator's seed */
+  double lower;               /* starts == NULL: bounds of the draw / swarm */
+  double upper;
+  int32_t pso_iter;           /* starts == NULL: >= 0 PSO iterations, < 0 uniform */
+  int32_t required_converged; /* stop-early threshold of this class */
+  int32_t layout;             /* ZEUS_LAYOUT_* */
+  int32_t tile;               /* tile width for ZEUS_LAYOUT_TILE */
+} zeus_host_class;
+
+typedef struct zeus_batch_plan zeus_batch_plan;
+int zeus_batch_plan_create(const zeus_host_class* classes, int32_t n_classes,
+                           const zeus_bfgs_config* config, zeus_batch_plan** plan);
+int zeus_batch_plan_run(zeus_batch_plan* plan, const zeus_host_class* classes,
+                        zeus_result* best, double* best_x, zeus_census* census,
+                        void* stream);
+/* Bytes the last run copied host-to-device, and the bytes every run copies
+ * back. */
+int zeus_batch_plan_traffic(const zeus_batch_plan* plan, size_t* h2d_bytes,
+                            size_t* d2h_bytes);
+int zeus_batch_plan_destroy(zeus_batch_plan* plan);
+
 /* ---- fit sensitivities ----------------------------------------------------
  * No counterpart in the reference (its dijet fit stops at the minimum,
  * examples/fit_dijet_spectrum.cu:162-221).  For a Poisson NLL batch with

@@ -147,6 +147,22 @@ class BatchClass(C.Structure):
     ]
 
 
+class HostClass(C.Structure):
+    _fields_ = [
+        ("problem", Problem),
+        ("n", C.c_int64),
+        ("runs_per_instance", C.c_int64),
+        ("starts", C.c_void_p),
+        ("seed", C.c_uint64),
+        ("lower", C.c_double),
+        ("upper", C.c_double),
+        ("pso_iter", C.c_int32),
+        ("required_converged", C.c_int32),
+        ("layout", C.c_int32),
+        ("tile", C.c_int32),
+    ]
+
+
 # Every symbol include/zeus_b200.h declares: (name, restype, argtypes).
 _P = C.c_void_p
 SIGNATURES = {
@@ -206,6 +222,15 @@ SIGNATURES = {
     "zeus_batch_device": (
         C.c_int, [C.POINTER(BatchClass), C.c_int32, C.POINTER(BfgsConfig), _P, C.c_size_t,
                   _P]),
+    "zeus_batch_plan_create": (
+        C.c_int, [C.POINTER(HostClass), C.c_int32, C.POINTER(BfgsConfig),
+                  C.POINTER(C.c_void_p)]),
+    "zeus_batch_plan_run": (
+        C.c_int, [C.c_void_p, C.POINTER(HostClass), C.POINTER(CResult), _P,
+                  C.POINTER(CCensus), _P]),
+    "zeus_batch_plan_traffic": (
+        C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "zeus_batch_plan_destroy": (C.c_int, [C.c_void_p]),
     "zeus_nll_sensitivity_device": (
         C.c_int, [C.POINTER(Problem), C.c_int64, C.c_int64, _P, _P, _P, _P, _P]),
     "zeus_write_trajectory_tsv": (
@@ -505,3 +530,96 @@ __all__ = [
     "PRNGType", "sobol_directions",
     "batch_device", "autotune", "BatchJob",
 ]
+
+
+class BatchPlan:
+    """Several objectives in one persistent kernel launch, host buffers in and
+    out: zeus_batch_plan_* (the batch form of zeus::Zeus).
+
+    ``classes`` is a list of dicts: ``obj`` (an Objective whose data/idata
+    hold every instance), ``n``, and either ``starts`` (host (n, dim) float64
+    array) or ``seed`` / ``lower`` / ``upper`` / ``pso_iter`` (starts drawn
+    on the device: PSO for pso_iter >= 0, else uniform Philox); optional
+    ``runs_per_instance``, ``required`` (stop-early threshold, default off),
+    ``layout``, ``tile``.  Device memory is allocated once, on the current
+    device; ``run()`` copies the host inputs in and returns one Result per
+    class, synchronously.  Pass pinned arrays (e.g. torch ``pin_memory()``
+    views) for asynchronous copies."""
+
+    def __init__(self, classes, max_iter: int = 10000, tol: float = 1e-8,
+                 block: int = 0, flags: int = 0):
+        self.specs = [dict(c) for c in classes]
+        self.cfg = make_config(max_iter, 1, tol, "fast", "adjoint", block=block, flags=flags)
+        self._keep = []
+        arr = self._host_classes(self.specs)
+        h = C.c_void_p()
+        check(lib().zeus_batch_plan_create(arr, len(self.specs), C.byref(self.cfg),
+                                           C.byref(h)))
+        self.handle = h
+        self.dims = [c["obj"].dim for c in self.specs]
+
+    def _host_classes(self, specs):
+        keep = []
+        arr = (HostClass * len(specs))()
+        for i, c in enumerate(specs):
+            obj = c["obj"]
+            d = None if obj.data is None else np.ascontiguousarray(obj.data, np.float64)
+            k = None if obj.idata is None else np.ascontiguousarray(obj.idata, np.int32)
+            keep += [d, k]
+            prob = obj.problem(None if d is None else d.ctypes.data,
+                               None if k is None else k.ctypes.data)
+            rpi = int(c.get("runs_per_instance", 0))
+            if rpi and k is not None:
+                prob.ndata = len(k) // max(1, (c["n"] + rpi - 1) // rpi)
+            st = c.get("starts")
+            if st is not None:
+                st = np.ascontiguousarray(st, np.float64)
+                if st.shape != (c["n"], obj.dim):
+                    raise ValueError(f"class {i}: starts must have shape {(c['n'], obj.dim)}")
+                keep.append(st)
+            arr[i] = HostClass(prob, c["n"], rpi, None if st is None else st.ctypes.data,
+                               int(c.get("seed", 0)), float(c.get("lower", 0.0)),
+                               float(c.get("upper", 0.0)), int(c.get("pso_iter", -1)),
+                               int(c.get("required", c["n"] + 1)),
+                               int(c.get("layout", LAYOUT_AUTO)), int(c.get("tile", 0)))
+        self._keep = keep
+        return arr
+
+    def run(self, classes=None, stream=None):
+        """Runs the batch (optionally with new host inputs of the same
+        shapes); returns a list of Result, one per class."""
+        if classes is not None:
+            self.specs = [dict(c) for c in classes]
+        arr = self._host_classes(self.specs)
+        nc = len(self.specs)
+        best = (CResult * nc)()
+        cen = (CCensus * nc)()
+        bx = np.zeros(sum(self.dims))
+        sh = 0 if stream is None else int(getattr(stream, "cuda_stream", stream))
+        check(lib().zeus_batch_plan_run(self.handle, arr, best, bx.ctypes.data, cen, sh))
+        out, off = [], 0
+        for i, d in enumerate(self.dims):
+            b, c = best[i], cen[i]
+            out.append(Result(idx=b.idx, status=b.status, fval=b.fval,
+                              gradientNorm=b.gradient_norm,
+                              coordinates=bx[off:off + d].copy(), iter=b.iter,
+                              c=Convergence(c.actual, c.claimed, c.surrendered, c.stopped)))
+            off += d
+        return out
+
+    def traffic(self):
+        """(host-to-device bytes of the last run, device-to-host bytes of a run)."""
+        h, d = C.c_size_t(), C.c_size_t()
+        check(lib().zeus_batch_plan_traffic(self.handle, C.byref(h), C.byref(d)))
+        return h.value, d.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().zeus_batch_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -47,6 +47,7 @@ UNITS = [
     ("zb_noalloc.cu", ["-fmad=false"]),
     ("zb_fit.cu", []),
     ("zb_grad.cu", []),
+    ("zb_plan.cu", []),
     ("zb_traj.cu", []),
     ("zb_sobol.cu", []),
     ("zb_runtime.cu", []),
