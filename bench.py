@@ -147,7 +147,7 @@ class Job:
     in a persistent batch."""
 
     def __init__(self, name, obj_fn, n, lo, hi, pso_iter, max_iter, required, tol=1e-8,
-                 runs_per_instance=0, ref_runs=8):
+                 runs_per_instance=0, ref_runs=64):
         self.name, self.obj_fn, self.n = name, obj_fn, n
         self.lo, self.hi, self.pso_iter = lo, hi, pso_iter
         self.max_iter, self.required, self.tol = max_iter, required, tol

@@ -115,7 +115,7 @@ def test_reference_dijet_fit_program(cuda, tmp_path):
     with open(data / "dijet_spectrum.tsv", "w") as fh:
         fh.write("bin_low\tbin_high\tcounts\n")
         for a, b, c in zip(lo, hi, k):
-            fh.write(f"{a!r}\t{b!r}\t{c}\n")
+            fh.write(f"{float(a)!r}\t{float(b)!r}\t{int(c)}\n")
     work = tmp_path / "run"
     work.mkdir()
     n, max_iter = 64, 1000
@@ -152,7 +152,7 @@ def test_reference_gaussian_class(cuda, dim, n, pso, max_iter):
 def test_reference_loglikelihood_class(cuda, tmp_path):
     xk, k, _ = O.dijet_toy()
     f = tmp_path / "bins.txt"
-    f.write_text("".join(f"{int(c)} {v!r}\n" for c, v in zip(k, xk)))
+    f.write_text("".join(f"{int(c)} {float(v)!r}\n" for c, v in zip(k, xk)))
     n, pso, max_iter = 64, 10, 1000
     out = run("ref_objectives_test", "nll", f, n, pso, max_iter, 42)
     st, fv, gn, it, x = parse_result_line(out)
