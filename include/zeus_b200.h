@@ -80,6 +80,10 @@ extern "C" {
 #define ZEUS_LAYOUT_THREAD 1 /* one run per thread, H in registers */
 #define ZEUS_LAYOUT_TILE 2   /* one run per 2..32-lane tile, H rows per lane */
 #define ZEUS_LAYOUT_CTA 3    /* one run per CTA, H in shared memory */
+#define ZEUS_LAYOUT_ROWS 4   /* one run per group of S*dim threads, each holding
+                                a segment of one row of H in registers; several
+                                groups per block (dim 64: 128 threads; dim 128:
+                                384 or 512) */
 
 typedef struct zeus_problem {
   int32_t kind;         /* ZEUS_OBJ_* */

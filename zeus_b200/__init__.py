@@ -32,7 +32,7 @@ OBJ_ROSENBROCK, OBJ_RASTRIGIN, OBJ_ACKLEY, OBJ_GAUSSIAN, OBJ_POISSON_NLL = range
 PROBLEM_SYMMETRIC = 1
 MODE_EXACT, MODE_FAST = 0, 1
 GRAD_DUAL, GRAD_ADJOINT = 0, 1
-LAYOUT_AUTO, LAYOUT_THREAD, LAYOUT_TILE, LAYOUT_CTA = 0, 1, 2, 3
+LAYOUT_AUTO, LAYOUT_THREAD, LAYOUT_TILE, LAYOUT_CTA, LAYOUT_ROWS = 0, 1, 2, 3, 4
 FLAG_NO_FIXED_POINT = 1
 (GRADPATH_THREAD, GRADPATH_TILE, GRADPATH_TILE_GRAD, GRADPATH_CTA, GRADPATH_CTA_GRAD,
  GRADPATH_QUADRATIC) = range(6)

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "zb_batch.cuh"
+#include "zb_bfgs_rows.cuh"
 #include "zb_objective_visit.cuh"
 #include "zb_reduce.cuh"
 
@@ -29,6 +30,10 @@ namespace zb {
       if (layout == ZEUS_LAYOUT_TILE)
         return tile >= 2 && tile <= 32 && !(tile & (tile - 1)) &&
                ((batch_widths(kind, dim) >> __builtin_ctz((unsigned)tile)) & 1u);
+      if (layout == ZEUS_LAYOUT_ROWS) // H rows in registers, both block sizes
+        return dim >= kBatchRowMinDim && kind != ZEUS_OBJ_GAUSSIAN &&
+               kind != ZEUS_OBJ_POISSON_NLL && row_segments(dim, kBatchBlockSmall) > 0 &&
+               row_segments(dim, kBatchBlockLarge) > 0;
       if (layout == ZEUS_LAYOUT_CTA) // H in shared memory only
         return dim >= kBatchCtaMinDim && !cta_h_global(dim, kBatchBlockSmall) &&
                !cta_h_global(dim, kBatchBlockLarge) &&
@@ -68,7 +73,16 @@ namespace zb {
           return;
         }
       }
-      *layout = ZEUS_LAYOUT_CTA;
+      *layout = batch_layout_ok(kind, dim, ZEUS_LAYOUT_ROWS, 0) ? ZEUS_LAYOUT_ROWS
+                                                                 : ZEUS_LAYOUT_CTA;
+    }
+
+    // shared memory (doubles) of a row-layout class: its groups side by side
+    size_t
+    rows_doubles_rt(int d, int block)
+    {
+      const int s = row_segments(d, block);
+      return s > 0 ? (size_t)(block / (s * d)) * row_smem_doubles_rt(d, s) : 0;
     }
 
     int64_t
@@ -215,9 +229,12 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
         cta_doubles_rt(b.kind, b.dim, block) * sizeof(double) > 227 * 1024)
       block = kBatchBlockSmall; // its CTA classes fit at 384 (checked above)
   size_t smem_cta = 0;
-  for (const BatchClass& b : hc)
+  for (const BatchClass& b : hc) {
     if (b.layout == ZEUS_LAYOUT_CTA)
       smem_cta = std::max(smem_cta, cta_doubles_rt(b.kind, b.dim, block));
+    if (b.layout == ZEUS_LAYOUT_ROWS)
+      smem_cta = std::max(smem_cta, rows_doubles_rt(b.dim, block));
+  }
   // CTA classes first, smallest dimension (least work per run) first: a
   // batch lasts as long as its slowest run, and a class whose bulk finishes
   // early lets its stalled runs (those iterating to MAX_ITER) overlap the
@@ -225,7 +242,8 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
   // 44.0 ms largest-first, 40.0 ms smallest-first).  Then the tile/thread
   // classes, largest dimension first.
   std::stable_sort(hc.begin(), hc.end(), [](const BatchClass& a, const BatchClass& b) {
-    const int ka = a.layout == ZEUS_LAYOUT_CTA, kb = b.layout == ZEUS_LAYOUT_CTA;
+    const int ka = a.layout == ZEUS_LAYOUT_CTA || a.layout == ZEUS_LAYOUT_ROWS;
+    const int kb = b.layout == ZEUS_LAYOUT_CTA || b.layout == ZEUS_LAYOUT_ROWS;
     if (ka != kb)
       return ka > kb;
     return ka ? a.dim < b.dim : a.dim > b.dim;
@@ -245,8 +263,9 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
   // CTA classes', and what matters is that their longest runs start early)
   bool has_cta = false, has_warp = false;
   for (const BatchClass& b : hc) {
-    has_cta |= b.layout == ZEUS_LAYOUT_CTA;
-    has_warp |= b.layout != ZEUS_LAYOUT_CTA;
+    const bool blockwide = b.layout == ZEUS_LAYOUT_CTA || b.layout == ZEUS_LAYOUT_ROWS;
+    has_cta |= blockwide;
+    has_warp |= !blockwide;
   }
   constexpr int kEarlyDiv = 16;
   bt.early_b = has_cta && has_warp ? std::max(1, sm_count() / kEarlyDiv) : 0;

@@ -4,6 +4,7 @@
 #pragma once
 
 #include "zb_batch.cuh"
+#include "zb_bfgs_rows.cuh"
 #include "zb_objective_visit.cuh"
 
 namespace zb {
@@ -122,7 +123,39 @@ namespace zb {
     const bool early = (int)blockIdx.x < bt.early_b;
     for (int pass = 0; pass < 2; ++pass) {
       if ((pass == 0) != early) {
-        // phase A: CTA-layout classes, one run per block at a time
+        // phase A, row-layout classes: the block splits into groups of S*D
+        // threads, each taking runs from the class queue on its own
+        for (int ci = 0; ci < ncls; ++ci) {
+          const BatchClass c = classes[ci];
+          if (c.layout != ZEUS_LAYOUT_ROWS)
+            continue;
+          const BfgsParams prm{c.n, bt.max_iter, c.required, bt.tol, bt.flags};
+          batch_visit(c, [&](auto f) {
+            using F = decltype(f);
+            constexpr int D = (int)F::arity;
+            constexpr int S = row_segments(D, kBlock);
+            if constexpr (S > 0 && D >= kBatchRowMinDim && RowLayoutObjective<F>) {
+              constexpr int NT = S * D;
+              const int gi = (int)threadIdx.x / NT;
+              double* gsm = sm + (size_t)gi * row_smem_doubles<D, S>();
+              long long* slot =
+                reinterpret_cast<long long*>(gsm + row_smem_doubles<D, S>() - 2);
+              for (;;) {
+                if ((int)threadIdx.x % NT == 0)
+                  *slot = (long long)atomicAdd(c.queue, 1ull);
+                asm volatile("bar.sync %0, %1;" ::"r"(1 + gi), "n"(NT) : "memory");
+                const int64_t r = *slot;
+                asm volatile("bar.sync %0, %1;" ::"r"(1 + gi), "n"(NT) : "memory");
+                if (r >= c.n)
+                  break;
+                row_run<F, D, S, true>(instance_for(f, c, r), gsm, 1 + gi, gi * NT,
+                                       prm, c.starts + r * D, r, c.out, c.ctl);
+              }
+            }
+          });
+          __syncthreads();
+        }
+        // phase A, CTA-layout classes, one run per block at a time
         for (int ci = 0; ci < ncls; ++ci) {
           const BatchClass c = classes[ci];
           if (c.layout != ZEUS_LAYOUT_CTA)
@@ -161,7 +194,7 @@ namespace zb {
       double* warp_buf = sm + (size_t)(threadIdx.x >> 5) * stride;
       for (int ci = 0; ci < ncls; ++ci) {
         const BatchClass c = classes[ci];
-        if (c.layout == ZEUS_LAYOUT_CTA)
+        if (c.layout == ZEUS_LAYOUT_CTA || c.layout == ZEUS_LAYOUT_ROWS)
           continue;
         const BfgsParams prm{c.n, bt.max_iter, c.required, bt.tol, bt.flags};
         batch_visit(c, [&](auto f) {

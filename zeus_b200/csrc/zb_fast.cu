@@ -39,11 +39,11 @@ namespace zb {
     (void)gradient;
     return builtin_supported(kind, dim) &&
            (thread_layout_supported(kind, dim) || tile_widths(kind, dim) != 0 ||
-            cta_layout_supported(kind, dim));
+            cta_layout_supported(kind, dim) || rows_layout_supported(kind, dim));
   }
 
-  // Only the CTA layout needs one: its run queue, and past about D = 160
-  // the blocks' H slices.
+  // Only the CTA and row layouts need one: their run queue, and past about
+  // D = 160 the CTA blocks' H slices.
   size_t
   fast_workspace_bytes(const Objective& o, const zeus_bfgs_config& c,
                        int64_t n)
@@ -85,6 +85,10 @@ namespace zb {
         if (!cta_layout_supported(o.kind, o.dim))
           break;
         return launch_cta(o, c, prm, starts, out, ctl, ws, ws_bytes, st);
+      case ZEUS_LAYOUT_ROWS:
+        if (!rows_layout_supported(o.kind, o.dim))
+          break;
+        return launch_rows(o, c, prm, starts, out, ctl, ws, ws_bytes, st);
       default:
         break;
     }

@@ -2,6 +2,7 @@
 // about D = 160 in a global-memory slice per block taken from the caller's
 // workspace).
 #include "zb_bfgs_coop.cuh"
+#include "zb_bfgs_rows.cuh"
 #include "zb_objective_visit.cuh"
 
 namespace zb {
@@ -72,7 +73,87 @@ namespace zb {
       kern<<<grid, B, smem, st>>>(f, prm, starts, out, ctl, hws, queue);
       return cuda_fail(cudaGetLastError(), "CTA-layout BFGS launch");
     }
+    // the row layout standalone: one group per block
+    constexpr int kRowBlockCap = 384;
+
+    template <class F, int D, bool Adj>
+    int
+    launch_rows_one(const F& f, const BfgsParams& prm, const double* starts,
+                    const RunOut& out, Control* ctl, void* ws, size_t ws_bytes,
+                    cudaStream_t st)
+    {
+      constexpr int S = row_segments(D, kRowBlockCap), NT = S * D;
+      const size_t smem = sizeof(double) * row_smem_doubles<D, S>();
+      auto kern = bfgs_rows_kernel<F, D, S, Adj>;
+      int rc = cuda_fail(cudaFuncSetAttribute(
+                           kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem),
+                         "row-layout shared memory attribute");
+      if (rc)
+        return rc;
+      int per_sm = 0;
+      if ((rc = cuda_fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern,
+                                                                         NT, smem),
+                          "row-layout occupancy")))
+        return rc;
+      if (per_sm < 1) {
+        set_error("row layout: dim %d does not fit on an SM", D);
+        return ZEUS_E_UNSUPPORTED;
+      }
+      if (!ws || ws_bytes < kQueueBytes) {
+        set_error("row layout at dim %d: %zu workspace bytes needed, got %zu", D,
+                  kQueueBytes, ws_bytes);
+        return ZEUS_E_WORKSPACE;
+      }
+      auto* queue = static_cast<unsigned long long*>(ws);
+      if ((rc = cuda_fail(cudaMemsetAsync(queue, 0, sizeof *queue, st),
+                          "row-layout run queue reset")))
+        return rc;
+      const int64_t cap = (int64_t)sm_count() * per_sm;
+      const unsigned grid = (unsigned)(prm.n < cap ? prm.n : cap);
+      kern<<<grid, NT, smem, st>>>(f, prm, starts, out, ctl, queue);
+      return cuda_fail(cudaGetLastError(), "row-layout BFGS launch");
+    }
+
+    template <class F>
+    constexpr bool
+    rows_built()
+    {
+      constexpr int D = (int)F::arity;
+      return D >= 32 && RowLayoutObjective<F> && row_segments(D, kRowBlockCap) > 0;
+    }
   } // namespace
+
+  bool
+  rows_layout_supported(int kind, int dim)
+  {
+    if (!builtin_supported(kind, dim))
+      return false;
+    Objective o{kind, dim, nullptr, nullptr, 0, 0, nullptr};
+    return visit_objective(o, [](auto f) -> int {
+             return rows_built<decltype(f)>() ? 1 : 0;
+           }) == 1;
+  }
+
+  int
+  launch_rows(const Objective& o, const zeus_bfgs_config& c, const BfgsParams& prm,
+              const double* starts, const RunOut& out, Control* ctl, void* ws,
+              size_t ws_bytes, cudaStream_t st)
+  {
+    const bool adjoint = c.gradient == ZEUS_GRAD_ADJOINT;
+    return visit_objective(o, [&](auto f) -> int {
+      using F = decltype(f);
+      constexpr int D = (int)F::arity;
+      if constexpr (rows_built<F>()) {
+        if (adjoint)
+          return launch_rows_one<F, D, true>(f, prm, starts, out, ctl, ws, ws_bytes, st);
+        return launch_rows_one<F, D, false>(f, prm, starts, out, ctl, ws, ws_bytes, st);
+      } else {
+        set_error("row layout: kind %d dim %d not built", F::kind, D);
+        return ZEUS_E_UNSUPPORTED;
+      }
+    });
+  }
 
   bool
   cta_layout_supported(int kind, int dim)
@@ -87,8 +168,10 @@ namespace zb {
   size_t
   cta_workspace_bytes(int dim, int64_t n)
   {
-    if (dim < kMinCtaDim || n <= 0)
+    if (dim < 32 || n <= 0)
       return 0;
+    if (dim < kMinCtaDim) // the row layout's run queue
+      return kQueueBytes;
     const int b = dim <= 64 ? 256 : 512;
     return kQueueBytes +
            (cta_h_global(dim, b)

@@ -224,4 +224,102 @@ namespace zb {
     }
   };
 
+  // A group of NT threads (NT a multiple of 32, starting at a warp
+  // boundary `base`) inside a larger block, synchronised by the named
+  // barrier `bar` (1..15; 0 is __syncthreads), so that several groups of a
+  // block run independent optimisations.  Same interface as CtaGroup;
+  // `red` holds row_red_doubles(NT / 32) doubles of shared memory.
+  __host__ __device__ constexpr int
+  row_red_doubles(int nw)
+  {
+    return 2 * 8 * nw + 8 + 8;
+  }
+
+  template <int NT>
+  struct RowGroup {
+    static_assert(NT % 32 == 0 && NT <= 1024, "a whole number of warps");
+    static constexpr int NW = NT / 32;
+    int base;
+    int bar;
+    double* red;
+    double* scratch;
+    mutable int parity = 0;
+
+    __device__ __forceinline__ int
+    rank() const
+    {
+      return (int)threadIdx.x - base;
+    }
+    static constexpr int
+    size()
+    {
+      return NT;
+    }
+    __device__ __forceinline__ void
+    sync() const
+    {
+      if constexpr (NT == 32)
+        __syncwarp();
+      else
+        asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(NT) : "memory");
+    }
+    template <int K>
+    __device__ __forceinline__ void
+    sum(double (&v)[K]) const
+    {
+      using RS = ReduceScatter<K>;
+      const auto shx = [](double x, int m) {
+        return __shfl_xor_sync(0xffffffffu, x, m);
+      };
+      const int t = rank(), lane = t & 31, warp = t >> 5;
+      double* buf = red + parity * (8 * NW);
+      double* tot = red + 2 * 8 * NW;
+      parity ^= 1;
+      const int idx = RS::template index<32>(lane);
+      const bool owner = (lane & (32 / RS::P - 1)) == 0 && idx < K;
+      const double mine = RS::template run<32>(v, lane, shx);
+      if constexpr (NW == 1) {
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          v[k] = __shfl_sync(0xffffffffu, mine, RS::template owner<32>(k));
+        return;
+      } else {
+        if (owner)
+          buf[idx * NW + warp] = mine;
+        sync();
+        if (warp == 0) {
+          double w[K];
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+            w[k] = lane < NW ? buf[k * NW + lane] : 0.0;
+          const double tt = RS::template run<32>(w, lane, shx);
+          if (owner)
+            tot[idx] = tt;
+        }
+        sync();
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+          v[k] = tot[k];
+      }
+    }
+    __device__ __forceinline__ double
+    sum(double v) const
+    {
+      double a[1] = {v};
+      sum<1>(a);
+      return a[0];
+    }
+    __device__ __forceinline__ double
+    bcast(double v, int src) const
+    {
+      double* slot = red + 2 * 8 * NW + 8;
+      if (rank() == src)
+        slot[0] = v;
+      sync();
+      const double r = slot[0];
+      sync();
+      return r;
+    }
+  };
+
 } // namespace zb

@@ -80,8 +80,15 @@ namespace zb {
                  const BfgsParams& prm, const double* starts,
                  const RunOut& out, Control* ctl, void* ws, size_t ws_bytes,
                  cudaStream_t st);
-  // workspace of a CTA-layout launch (non-zero only when H is in global
-  // memory)
+  // the row layout (zb_bfgs_rows.cuh): one run per group of S*dim threads,
+  // H rows in registers
+  bool rows_layout_supported(int kind, int dim);
+  int launch_rows(const Objective& o, const zeus_bfgs_config& c,
+                  const BfgsParams& prm, const double* starts,
+                  const RunOut& out, Control* ctl, void* ws, size_t ws_bytes,
+                  cudaStream_t st);
+  // workspace of a CTA- or row-layout launch: the run queue, and past about
+  // D = 160 the CTA blocks' H slices
   size_t cta_workspace_bytes(int dim, int64_t n);
   // default layout / tile width for (kind, dim): ZEUS_LAYOUT_* and width
   void default_layout(int kind, int dim, int* layout, int* tile);

@@ -849,8 +849,8 @@ int
 zeus_autotune_record(int32_t kind, int32_t dim, int32_t gradient,
                      int32_t layout, int32_t tile)
 {
-  if (layout < ZEUS_LAYOUT_THREAD || layout > ZEUS_LAYOUT_CTA) {
-    set_error("zeus_autotune_record: layout must be THREAD, TILE or CTA");
+  if (layout < ZEUS_LAYOUT_THREAD || layout > ZEUS_LAYOUT_ROWS) {
+    set_error("zeus_autotune_record: layout must be THREAD, TILE, CTA or ROWS");
     return ZEUS_E_INVALID;
   }
   int dev = 0;
@@ -886,6 +886,8 @@ zeus_autotune(const zeus_problem* problem, const zeus_bfgs_config* config,
       cand.push_back({ZEUS_LAYOUT_TILE, 1 << k});
   if (cta_layout_supported(kind, dim))
     cand.push_back({ZEUS_LAYOUT_CTA, 0});
+  if (rows_layout_supported(kind, dim))
+    cand.push_back({ZEUS_LAYOUT_ROWS, 0});
   if (cand.empty()) {
     set_error("zeus_autotune: no layout built for kind %d dim %d", kind, dim);
     return ZEUS_E_UNSUPPORTED;
@@ -909,6 +911,7 @@ zeus_autotune(const zeus_problem* problem, const zeus_bfgs_config* config,
   zeus_bfgs_config c0 = *config;
   c0.layout = ZEUS_LAYOUT_TILE; // any; the workspace does not depend on it
   const size_t wsz = zeus_bfgs_workspace_size(problem, &c0, n_sample);
+  // (CTA and row layouts: the same run queue)
   if ((rc = alloc(sizeof(double) * nd, &starts)) ||
       (rc = alloc(sizeof(double) * n_sample, &fval)) ||
       (rc = alloc(sizeof(int32_t) * n_sample, &status)) ||
