@@ -32,8 +32,8 @@ namespace zb {
                ((batch_widths(kind, dim) >> __builtin_ctz((unsigned)tile)) & 1u);
       if (layout == ZEUS_LAYOUT_ROWS) // H rows in registers, both block sizes
         return dim >= kBatchRowMinDim && kind != ZEUS_OBJ_GAUSSIAN &&
-               kind != ZEUS_OBJ_POISSON_NLL && row_segments(dim, kBatchBlockSmall) > 0 &&
-               row_segments(dim, kBatchBlockLarge) > 0;
+               kind != ZEUS_OBJ_POISSON_NLL && row_warps(dim, kBatchBlockSmall) > 0 &&
+               row_warps(dim, kBatchBlockLarge) > 0;
       if (layout == ZEUS_LAYOUT_CTA) // H in shared memory only
         return dim >= kBatchCtaMinDim && !cta_h_global(dim, kBatchBlockSmall) &&
                !cta_h_global(dim, kBatchBlockLarge) &&
@@ -81,8 +81,8 @@ namespace zb {
     size_t
     rows_doubles_rt(int d, int block)
     {
-      const int s = row_segments(d, block);
-      return s > 0 ? (size_t)(block / (s * d)) * row_smem_doubles_rt(d, s) : 0;
+      const int nw = row_warps(d, block);
+      return nw > 0 ? (size_t)(block / (32 * nw)) * row_smem_doubles_rt(d, nw) : 0;
     }
 
     int64_t

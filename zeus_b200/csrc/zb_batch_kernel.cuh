@@ -133,13 +133,13 @@ namespace zb {
           batch_visit(c, [&](auto f) {
             using F = decltype(f);
             constexpr int D = (int)F::arity;
-            constexpr int S = row_segments(D, kBlock);
-            if constexpr (S > 0 && D >= kBatchRowMinDim && RowLayoutObjective<F>) {
-              constexpr int NT = S * D;
+            constexpr int NW = row_warps(D, kBlock);
+            if constexpr (NW > 0 && D >= kBatchRowMinDim && RowLayoutObjective<F>) {
+              constexpr int NT = 32 * NW;
               const int gi = (int)threadIdx.x / NT;
-              double* gsm = sm + (size_t)gi * row_smem_doubles<D, S>();
+              double* gsm = sm + (size_t)gi * row_smem_doubles<D, NW>();
               long long* slot =
-                reinterpret_cast<long long*>(gsm + row_smem_doubles<D, S>() - 2);
+                reinterpret_cast<long long*>(gsm + row_smem_doubles<D, NW>() - 2);
               for (;;) {
                 if ((int)threadIdx.x % NT == 0)
                   *slot = (long long)atomicAdd(c.queue, 1ull);
@@ -148,7 +148,7 @@ namespace zb {
                 asm volatile("bar.sync %0, %1;" ::"r"(1 + gi), "n"(NT) : "memory");
                 if (r >= c.n)
                   break;
-                row_run<F, D, S, true>(instance_for(f, c, r), gsm, 1 + gi, gi * NT,
+                row_run<F, D, NW, true>(instance_for(f, c, r), gsm, 1 + gi, gi * NT,
                                        prm, c.starts + r * D, r, c.out, c.ctl);
               }
             }

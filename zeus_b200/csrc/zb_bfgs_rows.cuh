@@ -1,31 +1,36 @@
 // Fast BFGS with the inverse Hessian in registers, one optimisation per group
-// of NT = S * D threads (the "row" layout, for mid-to-large D where H fits
-// the register file: D = 64 at S = 2, D = 128 at S = 3 or 4).
+// of NW warps (the "row" layout, for D a multiple of 32 where H fits the
+// register file: D = 32 on 2 warps, 64 on 4, 128 on 12 or 16).
 //
-// Thread t of the group owns row r = t % D of H and segment c = t / D of
-// its columns, [c * CW, c * CW + CW), CW = ceil(D / S): CW doubles of H in
-// registers, no shared-memory traffic for H at all.  Several groups share a
-// block (named barriers 1..15), so that a block runs several independent
-// optimisations at once and the latency of one run's barriers and
-// reductions overlaps the others' arithmetic.
+// Warp w of the group owns column segment w of H, [w * CW, w * CW + CW)
+// with CW = ceil(D / NW), and lane l the R = D / 32 rows l*R .. l*R + R - 1:
+// R x CW doubles of H per thread, in registers, so H costs no
+// shared-memory traffic at all.  All lanes of a warp walk the same column,
+// so each column's four vector entries (s, w, y, g_x) are one broadcast
+// load serving R rows.  Several groups share a block (named barriers
+// 1..15), so that a block runs several independent optimisations at once
+// and one run's barriers and reductions overlap the others' arithmetic.
 //
 // An iteration (the reference's semantics, bfgs_sequential.cuh:99-219):
 //   1. line search: the group's warps split into trial groups of ST lanes,
 //      enough for all 21 trials (alpha = 2^-k, k = 0..20) in one round; each
-//      evaluates f at its materialised trial point; one barrier publishes
-//      the values and a ballot in every warp picks the first passing trial
-//      (c1 = 0.1, strict decrease; trial 20 is taken when none passes);
+//      evaluates f at its trial point, written from registers at a padded
+//      stride (the groups of a warp read different banks); one barrier
+//      publishes the values and a ballot in every warp picks the first
+//      passing trial (c1 = 0.1, strict decrease; trial 20 is taken when none
+//      passes);
 //   2. the gradient at the accepted point (its trial point, already in
 //      shared memory, is the same bits as fma(alpha, p, x));
 //   3. one pass over the registers: the previous iteration's deferred
 //      rank-2 update H_rj += s_r w_j + w_r s_j (two FMAs; each thread reads
-//      its row as a row, so exact symmetry is not needed) and the partial
-//      row sums of u = H y and h = H g_x; the S partials of a row meet in
-//      shared memory;
+//      its rows as rows, so exact symmetry is not needed) and the partial
+//      row sums of u = H y and h = H g_x; the NW segment partials of a row
+//      meet in shared memory;
 //   4. one group reduction of {s.y, y.u, u.g, s.g, g.h, g.g, stop}, from
 //      which p+ = -(h + s (w.g) + w (s.g)) and g.p+ follow without a
 //      second pass over H (w = hb s - rho u, rho = 1/s.y, hb = rho (1 +
 //      rho y.u) / 2); the update is skipped when |s.y| < 1e-14.
+// Thread t < D keeps coordinate t's scalars (x, p, s, w, y, g_x).
 // Accept-if-better, the fixed-point exit and the termination protocol are
 // those of the thread, tile and CTA layouts.
 #pragma once
@@ -44,73 +49,93 @@ namespace zb {
     return nw >= 21 ? 32 : 2 * nw >= 21 ? 16 : 4 * nw >= 21 ? 8 : 8 * nw >= 21 ? 4 : 2;
   }
 
-  // Shared memory of one group (doubles): x | p | g[2] | {s, w, y, g_x}[D]
-  // | row partial sums 2 x S x D (S > 1) | trial points NG x D | trial
-  // values 32 | reductions | scratch NT | run slot 2.  Every part is an
-  // even number of doubles, so the parts stay 16-byte aligned.
+  // Trial points are stored at a stride whose offset modulo 16 doubles (one
+  // pass over the 32 banks) equals the trial group's width: the ST-lane
+  // groups of a warp then read disjoint banks.
   __host__ __device__ constexpr int
-  row_smem_doubles_rt(int d, int s)
+  row_trial_stride(int d, int st)
   {
-    const int nt = s * d, nw = nt / 32, de = (d + 1) & ~1;
-    const int ng = nw * (32 / row_trial_width(nw));
-    return 4 * de + 4 * d + (s > 1 ? 2 * s * de : 0) + ng * de + 32 +
+    const int want = st % 16, have = d % 16;
+    return d + ((want - have + 16) % 16);
+  }
+
+  // Shared memory of one group (doubles): x | p | g[2] | {s, w, y, g_x}[D]
+  // | row partial sums 2 x NW x D | trial points NG at the padded stride |
+  // trial values 32 | reductions | scratch NT | run slot 2.  Every part is
+  // an even number of doubles, so the parts stay 16-byte aligned.
+  __host__ __device__ constexpr int
+  row_smem_doubles_rt(int d, int nw)
+  {
+    const int nt = 32 * nw, de = (d + 1) & ~1, st = row_trial_width(nw);
+    const int ng = nw * (32 / st);
+    return 4 * de + 4 * d + 2 * nw * de + ng * ((row_trial_stride(d, st) + 1) & ~1) + 32 +
            row_red_doubles(nw) + nt + 2;
   }
 
-  template <int D, int S>
+  template <int D, int NWG>
   struct RowShape {
-    static constexpr int NT = S * D;
-    static constexpr int NW = NT / 32;
-    static constexpr int CW = (D + S - 1) / S; // columns per segment
+    static constexpr int NW = NWG;
+    static constexpr int NT = 32 * NW;
+    static constexpr int R = D / 32;              // rows per lane
+    static constexpr int CW = (D + NW - 1) / NW;  // columns per warp
     static constexpr int ST = row_trial_width(NW);
     static constexpr int TPW = 32 / ST; // trial groups per warp
     static constexpr int NG = NW * TPW;
     static constexpr int DE = (D + 1) & ~1; // vector stride (16-byte aligned)
-    static_assert(NT % 32 == 0, "the group is a whole number of warps");
+    static constexpr int TSTR = (row_trial_stride(D, ST) + 1) & ~1;
+    static_assert(D % 32 == 0, "the rows split evenly over the lanes");
     static_assert(NG >= kLineSearchTrials + 1 && NG <= 32,
                   "one round of trial groups, judged by one ballot");
   };
 
-  template <int D, int S>
+  template <int D, int NW>
   __host__ __device__ constexpr int
   row_smem_doubles()
   {
-    return row_smem_doubles_rt(D, S);
+    return row_smem_doubles_rt(D, NW);
   }
 
   template <class F>
   concept RowLayoutObjective = !TrialsWithGradient<F>;
 
-  // One run on the group: `sm` holds row_smem_doubles<D, S>() doubles
-  // (16-byte aligned); the group is threads [base, base + S*D) of the
+  // One run on the group: `sm` holds row_smem_doubles<D, NW>() doubles
+  // (16-byte aligned); the group is threads [base, base + 32 NW) of the
   // block, synchronised by named barrier `bar`.
-  template <class F, int D, int S, bool Adjoint>
+  template <class F, int D, int NW, bool Adjoint>
   __device__ __forceinline__ void
   row_run(const F& f, double* sm, int bar, int base, const BfgsParams& prm,
           const double* __restrict__ x0, int64_t run, const RunOut& out,
           Control* ctl)
   {
-    using RS = RowShape<D, S>;
-    constexpr int NT = RS::NT, CW = RS::CW, ST = RS::ST, TPW = RS::TPW;
-    constexpr int DE = RS::DE;
+    using RS = RowShape<D, NW>;
+    constexpr int NT = RS::NT, R = RS::R, CW = RS::CW, ST = RS::ST, TPW = RS::TPW;
+    constexpr int DE = RS::DE, TSTR = RS::TSTR;
     double* X = sm;
     double* P = X + DE;
     double* G = P + DE; // two slots of DE
-    double* SWYG = G + 2 * DE;
-    double* PART = SWYG + 4 * D;
-    double* TX = PART + (S > 1 ? 2 * S * DE : 0);
-    double* TF = TX + RS::NG * DE;
+    // per-coordinate vectors of the H pass, {s, w} and {y, g_x} pairs, and
+    // the row partial sums [u | h][warp][.], all in owner order: coordinate
+    // r sits at oi(r) = (r % R) * 32 + r / R, so the owner of r (thread
+    // oi(r)) and each lane reading its R rows touch consecutive slots
+    double* SW = G + 2 * DE;
+    double* YG = SW + 2 * D;
+    double* PART = SW + 4 * D;
+    double* TX = PART + 2 * NW * DE;
+    double* TF = TX + RS::NG * TSTR;
     double* red = TF + 32;
-    double* scratch = red + row_red_doubles(RS::NW);
+    double* scratch = red + row_red_doubles(NW);
     const RowGroup<NT> grp{base, bar, red, scratch};
     const int t = grp.rank(), lw = t >> 5, lane = t & 31;
-    const int r = t % D, c = t / D, j0 = c * CW;
-    const bool owner = c == 0;
+    const int j0 = lw * CW, r0 = lane * R; // my columns and rows
+    const bool owner = t < D;              // thread oi(r) keeps coordinate r
+    const int r = owner ? (t % 32) * R + t / 32 : 0;
 
-    double H[CW];
+    double H[R][CW];
 #pragma unroll
-    for (int k = 0; k < CW; ++k)
-      H[k] = (j0 + k == r) ? 1.0 : 0.0;
+    for (int q = 0; q < R; ++q)
+#pragma unroll
+      for (int k = 0; k < CW; ++k)
+        H[q][k] = (j0 + k == r0 + q) ? 1.0 : 0.0;
     for (int i = t; i < D; i += NT)
       X[i] = x0[i];
     grp.sync();
@@ -126,14 +151,17 @@ namespace zb {
         v[0] = fma(gi, -gi, 0.0);
         P[r] = -gi;
       }
-      grp.template sum<2>(v); // its barriers publish p
+      grp.template sum<2>(v); // its barrier publishes p
       ddir = v[0];
       stop = v[1] != 0.0;
     }
     long long n_eval = 1, n_grad = 1;
     int status = kUnset, iter, executed = -1, cur = 0;
     double fout = best, gout = 0.0;
-    bool pend = false; // SWYG's {s, w} hold an update not yet applied to H
+    bool pend = false; // SW holds an update not yet applied to H
+    // the stop flag read in the previous iteration (a run sees the flag one
+    // iteration after it reads it, so the read's latency is off the path)
+    int stop_seen = 0;
 
     for (iter = 0; iter < prm.max_iter; ++iter) {
       if (stop) {
@@ -145,26 +173,40 @@ namespace zb {
       int found;
       double fnew;
       {
+        // this lane's coordinates of x and p, read once: the trial points
+        // are written from registers
+        constexpr int RV = (D + 31) / 32;
+        double xr[RV], pr[RV];
+#pragma unroll
+        for (int q = 0; q < RV; ++q) {
+          const int i = lane + 32 * q;
+          xr[q] = i < D ? X[i] : 0.0;
+          pr[q] = i < D ? P[i] : 0.0;
+        }
+        if (t == 0)
+          stop_now = load_stop(ctl);
         const int sub = lane / ST;
 #pragma unroll
         for (int q = 0; q < TPW; ++q) {
           const int k = lw * TPW + q;
           if (k <= kLineSearchTrials) {
             const double ak = pow2neg(k);
-            double* tx = TX + k * DE;
-            for (int i = lane; i < D; i += 32)
-              tx[i] = fma(ak, P[i], X[i]);
+            double* tx = TX + k * TSTR;
+#pragma unroll
+            for (int v = 0; v < RV; ++v) {
+              const int i = lane + 32 * v;
+              if (i < D)
+                tx[i] = fma(ak, pr[v], xr[v]);
+            }
           }
         }
         __syncwarp();
-        if (t == 0)
-          stop_now = load_stop(ctl);
         const int k = lw * TPW + sub;
         const TileGroup<ST> sg(cg::tiled_partition<ST>(cg::this_thread_block()),
                                scratch + lw * 32 + sub * ST);
         double f1 = 0.0;
         if (k <= kLineSearchTrials) // uniform within the trial group
-          f1 = coop_value<F, D>(f, sg, TX + k * DE);
+          f1 = coop_value<F, D>(f, sg, TX + k * TSTR);
         if (sg.rank() == 0)
           TF[k] = f1;
         grp.sync();
@@ -180,7 +222,7 @@ namespace zb {
         fnew = __shfl_sync(0xffffffffu, fk, found);
         n_eval += found + 1;
       }
-      const double* xa = TX + found * DE; // the accepted point
+      const double* xa = TX + found * TSTR; // the accepted point
       double* gn = G + (cur ^ 1) * DE;
       const double* g = G + cur * DE;
       coop_gradient_only<F, D, Adjoint>(f, grp, xa, gn);
@@ -193,53 +235,73 @@ namespace zb {
         s_r = xa[r] - X[r];
         y_r = gnr - go;
         gx_r = take ? gnr : go;
-        *reinterpret_cast<double2*>(SWYG + 4 * r + 2) = make_double2(y_r, gx_r);
+        *reinterpret_cast<double2*>(YG + 2 * t) = make_double2(y_r, gx_r);
       }
       grp.sync();
 
       // ---- the pass over H: deferred update, partial sums of H y and H g_x
-      double au[2] = {0.0, 0.0}, ah[2] = {0.0, 0.0};
-      {
-        const double2 swr = *reinterpret_cast<const double2*>(SWYG + 4 * r);
-        const double sr = swr.x, wr = swr.y;
-        if (pend) {
+      // over this warp's columns for this lane's rows
+      double au[R], ah[R];
 #pragma unroll
-          for (int k = 0; k < CW; ++k) {
-            const int j = j0 + k;
-            if (D % S == 0 || j < D) {
-              const double2 sw = *reinterpret_cast<const double2*>(SWYG + 4 * j);
-              const double2 yg = *reinterpret_cast<const double2*>(SWYG + 4 * j + 2);
-              H[k] = fma(sr, sw.y, fma(wr, sw.x, H[k]));
-              au[k & 1] = fma(H[k], yg.x, au[k & 1]);
-              ah[k & 1] = fma(H[k], yg.y, ah[k & 1]);
+      for (int q = 0; q < R; ++q) {
+        au[q] = 0.0;
+        ah[q] = 0.0;
+      }
+      if (pend) {
+        double sr[R], wr[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const double2 sw = *reinterpret_cast<const double2*>(SW + 2 * (q * 32 + lane));
+          sr[q] = sw.x;
+          wr[q] = sw.y;
+        }
+#pragma unroll
+        for (int k = 0; k < CW; ++k) {
+          const int j = j0 + k;
+          if (D % NW == 0 || j < D) {
+            const int oj = (j % R) * 32 + j / R;
+            const double2 sw = *reinterpret_cast<const double2*>(SW + 2 * oj);
+            const double2 yg = *reinterpret_cast<const double2*>(YG + 2 * oj);
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+              H[q][k] = fma(sr[q], sw.y, fma(wr[q], sw.x, H[q][k]));
+              au[q] = fma(H[q][k], yg.x, au[q]);
+              ah[q] = fma(H[q][k], yg.y, ah[q]);
             }
           }
-        } else {
+        }
+      } else {
 #pragma unroll
-          for (int k = 0; k < CW; ++k) {
-            const int j = j0 + k;
-            if (D % S == 0 || j < D) {
-              const double2 yg = *reinterpret_cast<const double2*>(SWYG + 4 * j + 2);
-              au[k & 1] = fma(H[k], yg.x, au[k & 1]);
-              ah[k & 1] = fma(H[k], yg.y, ah[k & 1]);
+        for (int k = 0; k < CW; ++k) {
+          const int j = j0 + k;
+          if (D % NW == 0 || j < D) {
+            const int oj = (j % R) * 32 + j / R;
+            const double2 yg = *reinterpret_cast<const double2*>(YG + 2 * oj);
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+              au[q] = fma(H[q][k], yg.x, au[q]);
+              ah[q] = fma(H[q][k], yg.y, ah[q]);
             }
           }
         }
       }
-      double uu = au[0] + au[1], hh = ah[0] + ah[1];
-      if constexpr (S > 1) {
-        PART[c * DE + r] = uu;
-        PART[(S + c) * DE + r] = hh;
-        grp.sync();
-        if (owner) {
-          uu = PART[r];
-          hh = PART[S * DE + r];
 #pragma unroll
-          for (int cc = 1; cc < S; ++cc) {
-            uu += PART[cc * DE + r];
-            hh += PART[(S + cc) * DE + r];
-          }
+      for (int q = 0; q < R; ++q) {
+        PART[lw * D + q * 32 + lane] = au[q];
+        PART[(NW + lw) * D + q * 32 + lane] = ah[q];
+      }
+      grp.sync();
+      double uu = 0.0, hh = 0.0;
+      if (owner) {
+        double u2[2] = {PART[t], NW > 1 ? PART[D + t] : 0.0};
+        double h2[2] = {PART[NW * D + t], NW > 1 ? PART[(NW + 1) * D + t] : 0.0};
+#pragma unroll
+        for (int w = 2; w < NW; ++w) {
+          u2[w & 1] += PART[w * D + t];
+          h2[w & 1] += PART[(NW + w) * D + t];
         }
+        uu = u2[0] + u2[1];
+        hh = h2[0] + h2[1];
       }
       double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
       if (owner) {
@@ -250,8 +312,9 @@ namespace zb {
         v[4] = gx_r * hh;
         v[5] = gx_r * gx_r;
       }
-      v[6] = (double)stop_now;
-      grp.template sum<7>(v); // every thread has finished reading SWYG's s, w
+      v[6] = (double)stop_seen;
+      stop_seen = stop_now;
+      grp.template sum<7>(v); // every thread has finished reading SW
       const bool skipped = fabs(v[0]) < kMinCurvature;
       const double sg = v[3], gh = v[4];
       double rho = 0.0, hb = 0.0, wg = 0.0;
@@ -264,7 +327,7 @@ namespace zb {
         if (!skipped) {
           const double wi = fma(hb, s_r, -rho * uu);
           P[r] = -(hh + s_r * wg + wi * sg);
-          *reinterpret_cast<double2*>(SWYG + 4 * r) = make_double2(s_r, wi);
+          *reinterpret_cast<double2*>(SW + 2 * t) = make_double2(s_r, wi);
         } else {
           P[r] = -hh;
         }
@@ -332,37 +395,49 @@ namespace zb {
     grp.sync(); // the group's shared memory is free for its next run
   }
 
-  // Segments per row for D in a block of `block` threads: the fewest that
-  // keep H's share per thread at most kRowMaxRegDoubles (so a thread's
-  // registers hold it beside the working set) and give whole warps
-  // dividing the block; 0 where none does.
+  // Warps of a group for D in a block of `block` threads: among the counts
+  // that divide the block, keep H's share per thread at most
+  // kRowMaxRegDoubles (so a thread's registers hold it beside the working
+  // set) and give the line search one round of trial groups, the fewest
+  // whose column segments split D evenly (no guarded tail), else the
+  // fewest; 0 where none fits (D not a multiple of 32, or too large).
   inline constexpr int kRowMaxRegDoubles = 48;
 
-  __host__ __device__ constexpr int
-  row_segments(int d, int block)
+  __host__ __device__ constexpr bool
+  row_warps_fit(int d, int block, int nw)
   {
-    for (int s = 1; s <= 8; ++s) {
-      const int nt = s * d, cw = (d + s - 1) / s;
-      if (nt % 32 == 0 && nt <= block && block % nt == 0 && cw <= kRowMaxRegDoubles &&
-          nt / 32 * (32 / 2) >= 21)
-        return s;
-    }
+    const int nt = 32 * nw, cw = (d + nw - 1) / nw;
+    return nt <= block && block % nt == 0 && (d / 32) * cw <= kRowMaxRegDoubles &&
+           nw * (32 / row_trial_width(nw)) >= kLineSearchTrials + 1;
+  }
+
+  __host__ __device__ constexpr int
+  row_warps(int d, int block)
+  {
+    if (d % 32 != 0)
+      return 0;
+    for (int nw = 1; nw <= 32; ++nw)
+      if (d % nw == 0 && row_warps_fit(d, block, nw))
+        return nw;
+    for (int nw = 1; nw <= 32; ++nw)
+      if (row_warps_fit(d, block, nw))
+        return nw;
     return 0;
   }
 
   // Standalone launches: one group per block, blocks take runs from the
   // workspace queue as they finish (block b starts with run b).
-  template <class F, int D, int S, bool Adjoint>
-  __global__ void __launch_bounds__(S * D)
+  template <class F, int D, int NW, bool Adjoint>
+  __global__ void __launch_bounds__(32 * NW)
     bfgs_rows_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
                      RunOut out, Control* ctl, unsigned long long* queue)
   {
     extern __shared__ __align__(16) double sm[];
-    constexpr int NT = S * D;
-    double* slot = sm + row_smem_doubles<D, S>() - 2;
+    constexpr int NT = 32 * NW;
+    double* slot = sm + row_smem_doubles<D, NW>() - 2;
     int64_t run = blockIdx.x;
     while (run < prm.n) {
-      row_run<F, D, S, Adjoint>(f, sm, 1, 0, prm, starts + run * D, run, out, ctl);
+      row_run<F, D, NW, Adjoint>(f, sm, 1, 0, prm, starts + run * D, run, out, ctl);
       if (threadIdx.x == 0)
         reinterpret_cast<long long*>(slot)[0] =
           (long long)gridDim.x + (long long)atomicAdd(queue, 1ull);

@@ -82,9 +82,9 @@ namespace zb {
                     const RunOut& out, Control* ctl, void* ws, size_t ws_bytes,
                     cudaStream_t st)
     {
-      constexpr int S = row_segments(D, kRowBlockCap), NT = S * D;
-      const size_t smem = sizeof(double) * row_smem_doubles<D, S>();
-      auto kern = bfgs_rows_kernel<F, D, S, Adj>;
+      constexpr int NW = row_warps(D, kRowBlockCap), NT = 32 * NW;
+      const size_t smem = sizeof(double) * row_smem_doubles<D, NW>();
+      auto kern = bfgs_rows_kernel<F, D, NW, Adj>;
       int rc = cuda_fail(cudaFuncSetAttribute(
                            kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem),
@@ -120,7 +120,7 @@ namespace zb {
     rows_built()
     {
       constexpr int D = (int)F::arity;
-      return D >= 32 && RowLayoutObjective<F> && row_segments(D, kRowBlockCap) > 0;
+      return D >= 32 && RowLayoutObjective<F> && row_warps(D, kRowBlockCap) > 0;
     }
   } // namespace
 

@@ -228,7 +228,10 @@ namespace zb {
   // boundary `base`) inside a larger block, synchronised by the named
   // barrier `bar` (1..15; 0 is __syncthreads), so that several groups of a
   // block run independent optimisations.  Same interface as CtaGroup;
-  // `red` holds row_red_doubles(NT / 32) doubles of shared memory.
+  // `red` holds row_red_doubles(NT / 32) doubles of shared memory.  A sum
+  // takes one barrier: each warp reduce-scatters its values and writes its
+  // partials (two buffers used in turn, as in CtaGroup), and after the
+  // barrier every lane adds up its value's partials itself, in warp order.
   __host__ __device__ constexpr int
   row_red_doubles(int nw)
   {
@@ -278,28 +281,35 @@ namespace zb {
       const int idx = RS::template index<32>(lane);
       const bool owner = (lane & (32 / RS::P - 1)) == 0 && idx < K;
       const double mine = RS::template run<32>(v, lane, shx);
+      (void)tot;
       if constexpr (NW == 1) {
 #pragma unroll
         for (int k = 0; k < K; ++k)
           v[k] = __shfl_sync(0xffffffffu, mine, RS::template owner<32>(k));
         return;
       } else {
+        // one barrier: every lane sums its value's per-warp partials in warp
+        // order (the same bits in every warp), then the totals go round the
+        // warp by shuffles
         if (owner)
           buf[idx * NW + warp] = mine;
         sync();
-        if (warp == 0) {
-          double w[K];
+        double tt = 0.0;
+        if (idx < K) {
+          const double* b = buf + idx * NW;
+          double a0 = b[0], a1 = NW > 1 ? b[1] : 0.0;
 #pragma unroll
-          for (int k = 0; k < K; ++k)
-            w[k] = lane < NW ? buf[k * NW + lane] : 0.0;
-          const double tt = RS::template run<32>(w, lane, shx);
-          if (owner)
-            tot[idx] = tt;
+          for (int w = 2; w + 1 < NW; w += 2) {
+            a0 += b[w];
+            a1 += b[w + 1];
+          }
+          if constexpr (NW > 2 && NW % 2 == 1)
+            a0 += b[NW - 1];
+          tt = a0 + a1;
         }
-        sync();
 #pragma unroll
         for (int k = 0; k < K; ++k)
-          v[k] = tot[k];
+          v[k] = __shfl_sync(0xffffffffu, tt, RS::template owner<32>(k));
       }
     }
     __device__ __forceinline__ double
