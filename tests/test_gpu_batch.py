@@ -129,7 +129,7 @@ def test_batch_rejects_bad_input(cuda):
                                        (zb.Rosenbrock(64), -5, 5)])
 def test_autotune_records_a_built_layout(cuda, obj, lo, hi):
     lay, tile, ms = zb.autotune(obj, n_sample=256, max_iter=300, lower=lo, upper=hi)
-    assert lay in (zb.LAYOUT_THREAD, zb.LAYOUT_TILE, zb.LAYOUT_CTA) and ms > 0
+    assert lay in (zb.LAYOUT_THREAD, zb.LAYOUT_TILE, zb.LAYOUT_CTA, zb.LAYOUT_ROWS) and ms > 0
     import ctypes as C
     l2, t2 = C.c_int32(), C.c_int32()
     assert zb.lib().zeus_autotune_lookup(obj.kind, obj.dim, zb.GRAD_ADJOINT, C.byref(l2),
