@@ -352,9 +352,13 @@ int zeus_nll_sensitivity_device(const zeus_problem* problem,
  * No reference counterpart (the reference fixes thread-per-run or a tile
  * of min(32, 2^floor(log2 D)) lanes, bfgs_parallel.cuh:57-65).  Times every
  * built layout / tile width for (problem, config) on n_sample uniform
- * starts in [lower, upper) and records the fastest in a per-process table
- * keyed by (device, kind, dim, gradient); ZEUS_LAYOUT_AUTO launches and
- * batches then use it.  Synchronous.  *best_ms is the winner's time. */
+ * starts in [lower, upper), and one run's iteration alone (200 iterations
+ * that neither converge nor stop early); a layout's estimate is the longer
+ * of the sample's time and max_iter of those iterations (a batch lasts as
+ * long as its slowest run, one that iterates to max_iter).  Records the
+ * layout with the lowest estimate in a per-process table keyed by (device,
+ * kind, dim, gradient); ZEUS_LAYOUT_AUTO launches and batches then use it.
+ * Synchronous.  *best_ms is the winner's estimate. */
 int zeus_autotune(const zeus_problem* problem, const zeus_bfgs_config* config,
                   int64_t n_sample, uint64_t seed, double lower, double upper,
                   int32_t* best_layout, int32_t* best_tile, float* best_ms,

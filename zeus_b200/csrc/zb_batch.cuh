@@ -4,12 +4,13 @@
 // and stop-early control; classes may have per-instance data (e.g. one toy
 // spectrum per 256 runs).  One block (512 or 384 threads) per SM:
 //
-//   phase A  first the row-layout classes (D = 64, 128: H rows in
-//            registers): the block splits into groups of S*D threads (three
-//            128-thread groups for D = 64 at 384 threads, the whole block for
-//            D = 128), each group taking runs from the class queue on its
-//            own; then the block takes runs of the CTA-layout classes (D > 32,
-//            H in shared memory) one at a time, smallest dimension first;
+//   phase A  first the row-layout classes (D = 32, 64, 128: H rows in
+//            registers): the block splits into groups of warps (six 2-warp
+//            groups for D = 32 and three 4-warp groups for D = 64 at 384
+//            threads, the whole block for D = 128), each group taking runs
+//            from the class queue on its own; then the block takes runs of
+//            the CTA-layout classes (D > 32, H in shared memory) one at a
+//            time, smallest dimension first;
 //   phase B  each warp, independently, walks the tile- and thread-layout
 //            classes: its tiles (or single threads) pop runs from the class
 //            queue as their previous run ends, so a slot is refilled the
@@ -87,8 +88,8 @@ namespace zb {
   }
   inline constexpr int kBatchThreadMaxDim = 4;
   inline constexpr int kBatchCtaMinDim = 33;
-  // the row layout in a batch (zb_bfgs_rows.cuh): dimensions 33 and up
-  inline constexpr int kBatchRowMinDim = 33;
+  // the row layout in a batch (zb_bfgs_rows.cuh): dimensions 32 and up
+  inline constexpr int kBatchRowMinDim = 32;
 
   // Objective with instance `inst`'s data: instances are stored one after
   // another (Gaussian: D*D doubles; NLL: ndata centres / counts, 4*ndata

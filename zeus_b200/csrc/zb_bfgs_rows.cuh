@@ -30,7 +30,8 @@
 //      which p+ = -(h + s (w.g) + w (s.g)) and g.p+ follow without a
 //      second pass over H (w = hb s - rho u, rho = 1/s.y, hb = rho (1 +
 //      rho y.u) / 2); the update is skipped when |s.y| < 1e-14.
-// Thread t < D keeps coordinate t's scalars (x, p, s, w, y, g_x).
+// Thread t < D (the first R warps) keeps the scalars of one coordinate
+// (x, p, s, w, y, g_x); only those warps take part in the group sums.
 // Accept-if-better, the fixed-point exit and the termination protocol are
 // those of the thread, tile and CTA layouts.
 #pragma once
@@ -98,6 +99,53 @@ namespace zb {
   template <class F>
   concept RowLayoutObjective = !TrialsWithGradient<F>;
 
+  // A RowGroup whose members are renumbered so that the member computing
+  // coordinate r of a cooperative gradient (rank r) is the thread that owns
+  // r: that thread then reads its entry back without a barrier.
+  template <int NT, int R>
+  struct OwnerGroup {
+    const RowGroup<NT>& g;
+    __device__ __forceinline__ int
+    rank() const
+    {
+      const int t = g.rank();
+      return t < 32 * R ? (t % 32) * R + t / 32 : t;
+    }
+    static constexpr int
+    size()
+    {
+      return NT;
+    }
+    __device__ __forceinline__ void
+    sync() const
+    {
+      g.sync();
+    }
+    template <int K>
+    __device__ __forceinline__ void
+    sum(double (&v)[K]) const
+    {
+      g.template sum<K>(v);
+    }
+    __device__ __forceinline__ double
+    sum(double v) const
+    {
+      return g.sum(v);
+    }
+    __device__ __forceinline__ double
+    bcast(double v, int src) const
+    {
+      return g.bcast(v, src);
+    }
+  };
+
+  // Objectives whose cooperative gradient has member r write entry r
+  // (coop_for over the group, or the dual passes): the owner's entry needs
+  // no barrier.
+  template <class F, class G, bool Adjoint>
+  concept OwnerWritesGradient =
+    !Adjoint || HasGradientCoop<F, G> || HasAdjointCoop<F, G>;
+
   // One run on the group: `sm` holds row_smem_doubles<D, NW>() doubles
   // (16-byte aligned); the group is threads [base, base + 32 NW) of the
   // block, synchronised by named barrier `bar`.
@@ -151,12 +199,13 @@ namespace zb {
         v[0] = fma(gi, -gi, 0.0);
         P[r] = -gi;
       }
-      grp.template sum<2>(v); // its barrier publishes p
+      grp.template sum<2, R>(v); // its barrier publishes p
       ddir = v[0];
       stop = v[1] != 0.0;
     }
     long long n_eval = 1, n_grad = 1;
     int status = kUnset, iter, executed = -1, cur = 0;
+    const double tol_sq4 = 4.0 * prm.tol * prm.tol;
     double fout = best, gout = 0.0;
     bool pend = false; // SW holds an update not yet applied to H
     // the stop flag read in the previous iteration (a run sees the flag one
@@ -225,9 +274,13 @@ namespace zb {
       const double* xa = TX + found * TSTR; // the accepted point
       double* gn = G + (cur ^ 1) * DE;
       const double* g = G + cur * DE;
-      coop_gradient_only<F, D, Adjoint>(f, grp, xa, gn);
+      {
+        const OwnerGroup<NT, R> og{grp};
+        coop_gradient_only<F, D, Adjoint>(f, og, xa, gn);
+        if constexpr (!OwnerWritesGradient<F, OwnerGroup<NT, R>, Adjoint>)
+          grp.sync();
+      }
       ++n_grad;
-      grp.sync();
       const bool take = fnew < best;
       double s_r = 0.0, y_r = 0.0, gx_r = 0.0;
       if (owner) {
@@ -314,7 +367,7 @@ namespace zb {
       }
       v[6] = (double)stop_seen;
       stop_seen = stop_now;
-      grp.template sum<7>(v); // every thread has finished reading SW
+      grp.template sum<7, R>(v); // every thread has finished reading SW
       const bool skipped = fabs(v[0]) < kMinCurvature;
       const double sg = v[3], gh = v[4];
       double rho = 0.0, hb = 0.0, wg = 0.0;
@@ -341,19 +394,20 @@ namespace zb {
         best = fnew;
         cur ^= 1;
       }
-      const double gnrm = sqrt(v[5]);
-      if (!isfinite(gnrm) || !isfinite(fnew)) {
+      // ||g|| = sqrt(g.g): taken only where it decides something (far
+      // above tol^2, g.g cannot pass the test)
+      if (!isfinite(v[5]) || !isfinite(fnew)) {
         status = kNonFinite;
         fout = fnew;
-        gout = gnrm;
+        gout = sqrt(v[5]);
         break;
       }
-      if (gnrm < prm.tol) {
+      if (v[5] <= tol_sq4 && sqrt(v[5]) < prm.tol) {
         if (t == 0)
           note_converged(ctl, prm.required);
         status = kConverged;
         fout = best;
-        gout = gnrm;
+        gout = sqrt(v[5]);
         break;
       }
       if (!take && skipped && !(prm.flags & kFlagNoFixedPoint)) {
@@ -372,7 +426,7 @@ namespace zb {
         const double gi = G[cur * DE + r];
         gg[0] = gi * gi;
       }
-      grp.template sum<1>(gg);
+      grp.template sum<1, R>(gg);
       gout = sqrt(gg[0]);
     }
     if (owner && out.x)

@@ -266,11 +266,14 @@ namespace zb {
       else
         asm volatile("bar.sync %0, %1;" ::"r"(bar), "n"(NT) : "memory");
     }
-    template <int K>
+    // AW: only warps below AW hold non-zero values (the others' partials
+    // are neither written nor read)
+    template <int K, int AW = NW>
     __device__ __forceinline__ void
     sum(double (&v)[K]) const
     {
       using RS = ReduceScatter<K>;
+      static_assert(AW >= 1 && AW <= NW, "active warps");
       const auto shx = [](double x, int m) {
         return __shfl_xor_sync(0xffffffffu, x, m);
       };
@@ -291,20 +294,20 @@ namespace zb {
         // one barrier: every lane sums its value's per-warp partials in warp
         // order (the same bits in every warp), then the totals go round the
         // warp by shuffles
-        if (owner)
+        if (owner && warp < AW)
           buf[idx * NW + warp] = mine;
         sync();
         double tt = 0.0;
         if (idx < K) {
           const double* b = buf + idx * NW;
-          double a0 = b[0], a1 = NW > 1 ? b[1] : 0.0;
+          double a0 = b[0], a1 = AW > 1 ? b[1] : 0.0;
 #pragma unroll
-          for (int w = 2; w + 1 < NW; w += 2) {
+          for (int w = 2; w + 1 < AW; w += 2) {
             a0 += b[w];
             a1 += b[w + 1];
           }
-          if constexpr (NW > 2 && NW % 2 == 1)
-            a0 += b[NW - 1];
+          if constexpr (AW > 2 && AW % 2 == 1)
+            a0 += b[AW - 1];
           tt = a0 + a1;
         }
 #pragma unroll

@@ -131,17 +131,34 @@ namespace zeus {
     }
 
     // Cooperative forms: member k takes terms / coordinates k, k+size, ...
+    // (for a group of compile-time size, alternating between two partial
+    // sums: the chain of dependent FMAs is half as long)
     template <class G>
     __device__ double
     value_coop(const G& grp, const double* x) const
     {
-      double part = 0.0;
-      detail::coop_for<(int)D - 1>(grp, [&](int i) {
-        const double t1 = 1.0 - x[i];
-        const double t2 = fma(-x[i], x[i], x[i + 1]);
-        part = fma(100.0 * t2, t2, fma(t1, t1, part));
-      });
-      return grp.sum(part);
+      if constexpr (requires { std::integral_constant<int, G::size()>{}; }) {
+        constexpr int S = G::size();
+        double acc[2] = {0.0, 0.0};
+#pragma unroll
+        for (int k = 0; k < ((int)D - 1 + S - 1) / S; ++k) {
+          const int i = grp.rank() + k * S;
+          if (i < (int)D - 1) {
+            const double t1 = 1.0 - x[i];
+            const double t2 = fma(-x[i], x[i], x[i + 1]);
+            acc[k & 1] = fma(100.0 * t2, t2, fma(t1, t1, acc[k & 1]));
+          }
+        }
+        return grp.sum(acc[0] + acc[1]);
+      } else {
+        double part = 0.0;
+        detail::coop_for<(int)D - 1>(grp, [&](int i) {
+          const double t1 = 1.0 - x[i];
+          const double t2 = fma(-x[i], x[i], x[i + 1]);
+          part = fma(100.0 * t2, t2, fma(t1, t1, part));
+        });
+        return grp.sum(part);
+      }
     }
     template <class G>
     __device__ double

@@ -1,5 +1,6 @@
 // C ABI (include/zeus_b200.h): validation, workspace layout, PSO graph
 // capture, reductions and the host-buffer orchestration of zeus_optimize.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -861,6 +862,9 @@ zeus_autotune_record(int32_t kind, int32_t dim, int32_t gradient,
   return ZEUS_OK;
 }
 
+// iterations of the autotuner's single-run latency measurement
+static constexpr int kTuneLatencyIters = 200;
+
 int
 zeus_autotune(const zeus_problem* problem, const zeus_bfgs_config* config,
               int64_t n_sample, uint64_t seed, double lower, double upper,
@@ -958,8 +962,37 @@ zeus_autotune(const zeus_problem* problem, const zeus_bfgs_config* config,
     }
     if (rc != ZEUS_OK)
       break;
-    if (ms_min < best) {
-      best = ms_min;
+    // the latency of one iteration of one run alone: a run that iterates to
+    // max_iter (one that neither converges nor reaches a fixed point) takes
+    // max_iter of them, and a batch lasts as long as its slowest run
+    float lat_ms = 0.f;
+    if (config->max_iter > 0) {
+      zeus_bfgs_config cl = c;
+      cl.max_iter = kTuneLatencyIters;
+      cl.tolerance = 0.0;                      // never converges
+      cl.flags |= ZEUS_FLAG_NO_FIXED_POINT;    // never stops early
+      cl.required_converged = 0x7fffffff;
+      for (int rep = 0; rep < 2 && rc == ZEUS_OK; ++rep) {
+        cudaMemsetAsync(ctl, 0, sizeof(int32_t) * 2, st);
+        cudaEventRecord(e0, st);
+        rc = zeus_bfgs_device(problem, &cl, static_cast<double*>(starts), 1, &ro,
+                              static_cast<int32_t*>(ctl), ws, wsz, st);
+        cudaEventRecord(e1, st);
+        if (rc == ZEUS_OK)
+          rc = cuda_fail(cudaEventSynchronize(e1), "autotune latency run");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0)
+          lat_ms = ms / kTuneLatencyIters;
+      }
+      if (rc != ZEUS_OK)
+        break;
+    }
+    // the class alone would take about the longer of its bulk (the sample)
+    // and one run iterating to max_iter
+    const float est = std::max(ms_min, lat_ms * (float)config->max_iter);
+    if (est < best) {
+      best = est;
       bl = layout;
       bt = tile;
     }
