@@ -215,13 +215,19 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
       warp_runs += (double)c.n / 32.0;
     hc.push_back(b);
   }
-  // Block size: 512 threads (16 warps per SM) when the tile/thread classes
-  // hold more than two waves of warps -- throughput -- else 384 (12 warps,
-  // 170 registers a thread instead of 128: faster per run, which is what a
-  // batch of long-running stragglers waits on).  config->block forces one.
+  // Block size: 512 threads (16 warps per SM) for a throughput batch -- only
+  // tile/thread classes, all of dimension 8 or less, more than two waves of
+  // warps (the dijet batch: 403 -> 360 ms) -- else 384 (12 warps, 170
+  // registers a thread instead of 128: faster per run, which is what a
+  // batch of long-running runs waits on; the multimodal batch 29.7 -> 26.1
+  // ms, the mixed one 23.1 -> 21.9 ms).  config->block forces one.
+  bool small_warp_only = true;
+  for (const BatchClass& b : hc)
+    small_warp_only &= (b.layout == ZEUS_LAYOUT_TILE || b.layout == ZEUS_LAYOUT_THREAD) &&
+                       b.dim <= 8;
   int block = config->block == kBatchBlockLarge || config->block == kBatchBlockSmall
                 ? config->block
-                : (warp_runs > 2.0 * sm_count() * (kBatchBlockLarge / 32)
+                : (small_warp_only && warp_runs > 2.0 * sm_count() * (kBatchBlockLarge / 32)
                      ? kBatchBlockLarge
                      : kBatchBlockSmall);
   for (const BatchClass& b : hc)

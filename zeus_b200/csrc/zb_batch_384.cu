@@ -6,7 +6,11 @@ namespace zb {
   int
   launch_batch_384(const BatchTable& bt, size_t smem, cudaStream_t st)
   {
-    return launch_batch_kernel<384>(bt, smem, st);
+    // the warp-sized bodies inlined where no row or CTA class is present
+    for (int i = 0; i < bt.ncls; ++i)
+      if (bt.c[i].layout == ZEUS_LAYOUT_CTA || bt.c[i].layout == ZEUS_LAYOUT_ROWS)
+        return launch_batch_kernel<384, false>(bt, smem, st);
+    return launch_batch_kernel<384, true>(bt, smem, st);
   }
 
 } // namespace zb
