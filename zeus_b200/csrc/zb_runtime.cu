@@ -304,6 +304,45 @@ namespace zb {
       return *t;
     }
 
+    // The library's own stream-ordered memory pool per device, for the
+    // buffers a host-buffer call (zeus_optimize, the autotuner) allocates
+    // and frees each time: its release threshold keeps the memory reserved
+    // between calls, so a repeated call maps nothing new (the device's
+    // default pool returns freed memory at every synchronisation, and the
+    // next call's allocations then cost milliseconds).  The pool is never
+    // destroyed; what it holds is at most the largest call's buffers.
+    int
+    pool_alloc(void** out, size_t bytes, cudaStream_t st)
+    {
+      static std::mutex mu;
+      static std::map<int, cudaMemPool_t> pools;
+      int dev = 0;
+      cudaError_t e = cudaGetDevice(&dev);
+      if (e != cudaSuccess)
+        return cuda_fail(e, "current device");
+      cudaMemPool_t pool = nullptr;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        auto it = pools.find(dev);
+        if (it == pools.end()) {
+          cudaMemPoolProps props{};
+          props.allocType = cudaMemAllocationTypePinned;
+          props.handleTypes = cudaMemHandleTypeNone;
+          props.location.type = cudaMemLocationTypeDevice;
+          props.location.id = dev;
+          if ((e = cudaMemPoolCreate(&pool, &props)) != cudaSuccess)
+            return cuda_fail(e, "memory pool");
+          uint64_t keep = ~0ull;
+          cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+          pools[dev] = pool;
+        } else {
+          pool = it->second;
+        }
+      }
+      return cuda_fail(cudaMallocFromPoolAsync(out, bytes ? bytes : 1, pool, st),
+                       "allocation");
+    }
+
     // Cached executable graphs for the PSO loop, keyed by the launch shape;
     // new pointer arguments go in through cudaGraphExecUpdate.
     struct GraphCache {
@@ -675,7 +714,7 @@ zeus_optimize(const zeus_problem* hp, double lower, double upper, int64_t n,
     *out = nullptr;
     if (bytes == 0)
       return ZEUS_OK;
-    const int r = cuda_fail(cudaMallocAsync(out, bytes, st), "allocation");
+    const int r = pool_alloc(out, bytes, st);
     if (r == ZEUS_OK)
       allocs.push_back(*out);
     return r;
@@ -904,8 +943,7 @@ zeus_autotune(const zeus_problem* problem, const zeus_bfgs_config* config,
     cudaStreamSynchronize(st);
   };
   auto alloc = [&](size_t bytes, void** out) -> int {
-    const int r = cuda_fail(cudaMallocAsync(out, bytes ? bytes : 1, st),
-                            "autotune allocation");
+    const int r = pool_alloc(out, bytes, st);
     if (r == ZEUS_OK)
       allocs.push_back(*out);
     return r;
