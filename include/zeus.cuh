@@ -101,15 +101,30 @@ namespace zeus {
 
   namespace detail {
 
+    // A call's device buffers and its own stream (the legacy stream cannot
+    // be captured into a graph; it is used only if no stream can be made).
     struct DeviceBuffers {
       std::vector<void*> p;
       cudaStream_t st = nullptr;
+      bool own = false;
+      DeviceBuffers()
+      {
+        own = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
+        if (!own) {
+          cudaGetLastError();
+          st = nullptr;
+        }
+      }
       ~DeviceBuffers()
       {
         for (void* q : p)
           cudaFreeAsync(q, st);
         cudaStreamSynchronize(st);
+        if (own)
+          cudaStreamDestroy(st);
       }
+      DeviceBuffers(const DeviceBuffers&) = delete;
+      DeviceBuffers& operator=(const DeviceBuffers&) = delete;
       template <class T>
       T*
       alloc(std::size_t n)
@@ -122,6 +137,61 @@ namespace zeus {
         return static_cast<T*>(q);
       }
     };
+
+    // The PSO (the reference's zeus.cuh:64-92 with pso.cuh's kernels): a
+    // thread per particle for D <= 32, a warp per particle above (its lanes
+    // move the D coordinates of one particle, coalesced; the same random
+    // counters and update expressions, so the same swarm).  The iterations
+    // are captured into one CUDA graph and launched once.
+    template <class Function, std::size_t D>
+    cudaError_t
+    run_pso(const Function& f, int64_t n, double lower, double upper, int iters,
+            uint64_t seed, const zb::PsoWork& w, double* starts, double* pbf,
+            cudaStream_t st, cudaEvent_t after_init)
+    {
+      const unsigned blocks = (unsigned)zb::pso_blocks(n, (int)D);
+      constexpr bool coop = (int)D >= zb::kPsoCoopMinDim;
+      zb::pso_reset_kernel<(int)D><<<1, 256, 0, st>>>(w);
+      if constexpr (coop)
+        zb::pso_init_coop_kernel<Function, (int)D>
+          <<<blocks, zb::kPsoBlock, 0, st>>>(f, n, lower, upper, seed, w, starts, pbf);
+      else
+        zb::pso_init_kernel<Function, (int)D>
+          <<<blocks, zb::kPsoBlock, 0, st>>>(f, n, lower, upper, seed, w, starts, pbf);
+      cudaError_t e = cudaGetLastError();
+      cudaEventRecord(after_init, st);
+      if (e != cudaSuccess || iters <= 0)
+        return e;
+      const auto iterations = [&] {
+        for (int t = 1; t <= iters; ++t) {
+          if constexpr (coop)
+            zb::pso_iter_coop_kernel<Function, (int)D><<<blocks, zb::kPsoBlock, 0, st>>>(
+              f, n, 0.5, 1.2, 1.5, seed, t, w, starts, pbf);
+          else
+            zb::pso_iter_kernel<Function, (int)D><<<blocks, zb::kPsoBlock, 0, st>>>(
+              f, n, 0.5, 1.2, 1.5, seed, t, w, starts, pbf);
+        }
+      };
+      if (!st) {
+        iterations();
+        return cudaGetLastError();
+      }
+      if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+        return e;
+      iterations();
+      cudaGraph_t g = nullptr;
+      cudaGraphExec_t ge = nullptr;
+      e = cudaStreamEndCapture(st, &g);
+      if (e == cudaSuccess)
+        e = cudaGraphInstantiate(&ge, g, 0);
+      if (e == cudaSuccess)
+        e = cudaGraphLaunch(ge, st);
+      if (ge)
+        cudaGraphExecDestroy(ge); // freed once the launch completes
+      if (g)
+        cudaGraphDestroy(g);
+      return e;
+    }
 
     // hws: for the CTA layout past about D = 160, a device buffer of
     // cta_h_slices(n) * D * D doubles holding each block's H
@@ -231,7 +301,7 @@ namespace zeus {
       zeus_census* cen = b.alloc<zeus_census>(1);
       cudaMemsetAsync(ctl, 0, 2 * sizeof(int32_t), b.st);
       if (PSO_ITER >= 0) {
-        const int64_t blocks = (n + zb::kPsoBlock - 1) / zb::kPsoBlock;
+        const int64_t blocks = zb::pso_blocks(n, (int)D);
         zb::PsoWork w;
         w.X = b.alloc<double>(N * D);
         w.V = b.alloc<double>(N * D);
@@ -244,16 +314,10 @@ namespace zeus {
           throw cudaErrorLaunchFailure;
         double* pbf = b.alloc<double>(N);
         cudaEventRecord(p0, b.st);
-        zb::pso_reset_kernel<(int)D><<<1, 256, 0, b.st>>>(w);
-        zb::pso_init_kernel<Function, (int)D>
-          <<<(unsigned)blocks, zb::kPsoBlock, 0, b.st>>>(f, n, lower, upper,
-                                                         (uint64_t)seed, w,
-                                                         starts, pbf);
-        cudaEventRecord(p1, b.st);
-        for (int t = 1; t <= PSO_ITER; ++t)
-          zb::pso_iter_kernel<Function, (int)D>
-            <<<(unsigned)blocks, zb::kPsoBlock, 0, b.st>>>(
-              f, n, 0.5, 1.2, 1.5, (uint64_t)seed, t, w, starts, pbf);
+        const cudaError_t pe = detail::run_pso<Function, D>(
+          f, n, lower, upper, PSO_ITER, (uint64_t)seed, w, starts, pbf, b.st, p1);
+        if (pe != cudaSuccess)
+          throw pe;
         cudaEventRecord(p2, b.st);
       } else if (zeus_starts((uint64_t)seed, prng, n, (int32_t)D, lower, upper,
                              starts, b.st) != ZEUS_OK) {

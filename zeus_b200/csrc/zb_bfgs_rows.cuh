@@ -34,6 +34,13 @@
 // (x, p, s, w, y, g_x); only those warps take part in the group sums.
 // Accept-if-better, the fixed-point exit and the termination protocol are
 // those of the thread, tile and CTA layouts.
+//
+// That is row_run_points.  For objectives with line forms (value terms and
+// gradient entries read from {x_i, p_i}, e.g. Rosenbrock) and D <= 64,
+// row_run_line stores no trial points: trial groups evaluate f(x + a p)
+// from {x, p}, every warp computes the gradient entries it needs itself,
+// and the row partials and dot products share one reduction -- three group
+// barriers an iteration instead of five.
 #pragma once
 
 #include "zb_bfgs_coop.cuh"
@@ -146,14 +153,15 @@ namespace zb {
   concept OwnerWritesGradient =
     !Adjoint || HasGradientCoop<F, G> || HasAdjointCoop<F, G>;
 
-  // One run on the group: `sm` holds row_smem_doubles<D, NW>() doubles
-  // (16-byte aligned); the group is threads [base, base + 32 NW) of the
-  // block, synchronised by named barrier `bar`.
+  // One run on the group, trial points stored: `sm` holds
+  // row_smem_doubles<D, NW>() doubles (16-byte aligned); the group is
+  // threads [base, base + 32 NW) of the block, synchronised by named
+  // barrier `bar`.
   template <class F, int D, int NW, bool Adjoint>
   __device__ __forceinline__ void
-  row_run(const F& f, double* sm, int bar, int base, const BfgsParams& prm,
-          const double* __restrict__ x0, int64_t run, const RunOut& out,
-          Control* ctl)
+  row_run_points(const F& f, double* sm, int bar, int base, const BfgsParams& prm,
+                 const double* __restrict__ x0, int64_t run, const RunOut& out,
+                 Control* ctl)
   {
     using RS = RowShape<D, NW>;
     constexpr int NT = RS::NT, R = RS::R, CW = RS::CW, ST = RS::ST, TPW = RS::TPW;
@@ -447,6 +455,349 @@ namespace zb {
       }
     }
     grp.sync(); // the group's shared memory is free for its next run
+  }
+
+  // Objectives whose value along the search line and whose gradient entries
+  // are read from {x_i, p_i} pairs in owner order (slot (i % R) * 32 + i /
+  // R; coordinate i of x + a p is fma(a, p_i, x_i), the bits of a stored
+  // trial point): member m of an S-lane trial group returns its partial sum
+  // of the value's terms, and gradient entry i needs only a few
+  // coordinates, so any thread computes the entries it uses itself.
+  template <class F>
+  concept RowLineObjective = requires(const F& f, const double2* xp, double a, int i) {
+    { f.template value_line_part<8, 1>(xp, a, i) } -> std::convertible_to<double>;
+    { f.template gradient_line_entry<1>(xp, a, i) } -> std::convertible_to<double>;
+  };
+
+  // Shared memory of row_run_line (doubles): {x, p}[D] | {s, w}[D] | per
+  // warp {y, g_x}[D] | row partial sums 2 x NW x D | trial values 32 |
+  // reductions | scratch NT; all vectors in owner order; within
+  // row_smem_doubles.
+  __host__ __device__ constexpr int
+  row_line_smem_doubles(int d, int nw)
+  {
+    const int de = (d + 1) & ~1;
+    return 2 * de + 2 * d + 2 * nw * d + 2 * nw * de + 32 + row_red_doubles(nw) + 32 * nw;
+  }
+
+  // One run on the group for a RowLineObjective with analytic gradients.
+  // Three barriers an iteration instead of five, and no trial points or
+  // gradients in shared memory:
+  //   1. line search: trial group k evaluates f(x + 2^-k p) from {x, p};
+  //      one barrier publishes the 21 values, a ballot picks the trial;
+  //   2. every lane computes the gradient entries at the accepted point of
+  //      its R rows, so each warp fills its own {y, g_x} table of all D
+  //      coordinates (no group barrier); gradients at x stay in registers
+  //      from one iteration to the next;
+  //   3. the pass over H (the previous iteration's deferred update, then
+  //      each warp's row partials of H y and H g_x, as in row_run_points);
+  //      the partials go to shared memory and the warp's share of y.Hy, g.Hy and
+  //      g.Hg (its rows' y and g_x times its column-segment partials) joins
+  //      s.y, s.g and g.g (warp 0) in ONE group reduction, whose barrier
+  //      also publishes the partials;
+  //   4. the owner of coordinate r adds up its row's NW partials, forms
+  //      p+_r and w_r and writes {x, p}[r] and {s, w}[r]; the end-of-
+  //      iteration barrier publishes them.
+  // The arithmetic of a run is that of row_run_points up to the order of
+  // the reductions' additions.
+  template <class F, int D, int NW>
+  __device__ __forceinline__ void
+  row_run_line(const F& f, double* sm, int bar, int base, const BfgsParams& prm,
+               const double* __restrict__ x0, int64_t run, const RunOut& out,
+               Control* ctl)
+  {
+    using RS = RowShape<D, NW>;
+    constexpr int NT = RS::NT, R = RS::R, CW = RS::CW, ST = RS::ST, TPW = RS::TPW;
+    constexpr int DE = RS::DE;
+    static_assert(row_line_smem_doubles(D, NW) <= row_smem_doubles<D, NW>() - 2,
+                  "fits the row layout's shared memory, run slot excluded");
+    double2* XP = reinterpret_cast<double2*>(sm); // {x, p}, owner order
+    double* SW = sm + 2 * DE;                      // {s, w}, owner order
+    double* YGW = SW + 2 * D; // warp w's {y, g_x} at YGW + 2 D w, owner order
+    double* PART = YGW + 2 * D * NW;
+    double* TF = PART + 2 * NW * DE;
+    double* red = TF + 32;
+    double* scratch = red + row_red_doubles(NW);
+    const RowGroup<NT> grp{base, bar, red, scratch};
+    const int t = grp.rank(), lw = t >> 5, lane = t & 31;
+    const int j0 = lw * CW, r0 = lane * R;
+    // warps 0..R-1: thread t keeps coordinate r, whose slot is t
+    const bool owner = t < D;
+    const int r = owner ? lane * R + lw : 0;
+
+    double H[R][CW];
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+#pragma unroll
+      for (int k = 0; k < CW; ++k)
+        H[q][k] = (j0 + k == r0 + q) ? 1.0 : 0.0;
+    // f and the gradient at the start, from a plain copy of x0
+    double* X0 = PART;
+    double* G0 = PART + DE;
+    for (int i = t; i < D; i += NT)
+      X0[i] = x0[i];
+    grp.sync();
+    double best = coop_value<F, D>(f, grp, X0);
+    coop_gradient_only<F, D, true>(f, grp, X0, G0);
+    grp.sync();
+    double gq[R]; // the gradient at x, this lane's rows
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+      gq[q] = G0[r0 + q];
+    double ddir;
+    bool stop;
+    {
+      double v[2] = {0.0, t == 0 ? (double)load_stop(ctl) : 0.0};
+      if (owner) {
+        const double gi = G0[r];
+        v[0] = fma(gi, -gi, 0.0);
+        XP[t] = make_double2(X0[r], -gi);
+      }
+      grp.template sum<2, R>(v); // its barrier publishes {x, p}
+      ddir = v[0];
+      stop = v[1] != 0.0;
+    }
+    long long n_eval = 1, n_grad = 1;
+    int status = kUnset, iter, executed = -1;
+    const double tol_sq4 = 4.0 * prm.tol * prm.tol;
+    double fout = best, gout = 0.0;
+    bool pend = false; // SW holds an update not yet applied to H
+    // the stop flag read in the previous iteration (a run sees the flag one
+    // iteration after it reads it, so the read's latency is off the path)
+    int stop_seen = 0;
+
+    for (iter = 0; iter < prm.max_iter; ++iter) {
+      if (stop) {
+        status = kStopped;
+        break;
+      }
+      int stop_now = 0;
+      if (t == 0)
+        stop_now = load_stop(ctl);
+      // ---- line search: trial k = TPW lw + (lane / ST) on ST lanes; the
+      // groups past trial 20 evaluate trial 20 again (no divergence) and
+      // their values are dropped
+      int found;
+      double fnew;
+      {
+        const int sub = lane / ST, k = lw * TPW + sub;
+        const int kk = k < kLineSearchTrials ? k : kLineSearchTrials;
+        double part = f.template value_line_part<ST, R>(XP, pow2neg(kk), lane % ST);
+#pragma unroll
+        for (int o = ST / 2; o >= 1; o >>= 1)
+          part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (lane % ST == 0 && k <= kLineSearchTrials)
+          TF[k] = part;
+        grp.sync();
+        bool pass = false;
+        double fk = 0.0;
+        if (lane <= kLineSearchTrials) {
+          fk = TF[lane];
+          const double ak = pow2neg(lane);
+          pass = lane == kLineSearchTrials ||
+                 (fk <= best + kArmijoC1 * ak * ddir && fk < best);
+        }
+        found = __ffs(__ballot_sync(0xffffffffu, pass)) - 1;
+        fnew = __shfl_sync(0xffffffffu, fk, found);
+        n_eval += found + 1;
+      }
+      const double alpha = pow2neg(found);
+      const bool take = fnew < best;
+      ++n_grad;
+      // ---- gradient entries at the accepted point for this lane's rows,
+      // into the warp's {y, g_x} table
+      double sq[R], yq[R], gxq[R];
+      double2 xpo = make_double2(0.0, 0.0); // the owner's {x, p}
+      double* yg_w = YGW + 2 * D * lw;
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const double2 c = XP[q * 32 + lane];
+        const double gn = f.template gradient_line_entry<R>(XP, alpha, r0 + q);
+        sq[q] = fma(alpha, c.y, c.x) - c.x;
+        yq[q] = gn - gq[q];
+        gxq[q] = take ? gn : gq[q];
+        *reinterpret_cast<double2*>(yg_w + 2 * (q * 32 + lane)) = make_double2(yq[q], gxq[q]);
+        if (q == lw)
+          xpo = c;
+      }
+      __syncwarp();
+
+      // ---- the pass over H: deferred update, partial sums of H y and H g_x
+      double au[R], ah[R];
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        au[q] = 0.0;
+        ah[q] = 0.0;
+      }
+      if (pend) {
+        double sr[R], wr[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const double2 sw = *reinterpret_cast<const double2*>(SW + 2 * (q * 32 + lane));
+          sr[q] = sw.x;
+          wr[q] = sw.y;
+        }
+#pragma unroll
+        for (int k = 0; k < CW; ++k) {
+          const int j = j0 + k;
+          if (D % NW == 0 || j < D) {
+            const int oj = (j % R) * 32 + j / R;
+            const double2 sw = *reinterpret_cast<const double2*>(SW + 2 * oj);
+            const double2 yg = *reinterpret_cast<const double2*>(yg_w + 2 * oj);
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+              H[q][k] = fma(sr[q], sw.y, fma(wr[q], sw.x, H[q][k]));
+              au[q] = fma(H[q][k], yg.x, au[q]);
+              ah[q] = fma(H[q][k], yg.y, ah[q]);
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < CW; ++k) {
+          const int j = j0 + k;
+          if (D % NW == 0 || j < D) {
+            const int oj = (j % R) * 32 + j / R;
+            const double2 yg = *reinterpret_cast<const double2*>(yg_w + 2 * oj);
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+              au[q] = fma(H[q][k], yg.x, au[q]);
+              ah[q] = fma(H[q][k], yg.y, ah[q]);
+            }
+          }
+        }
+      }
+      double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        PART[lw * DE + q * 32 + lane] = au[q];
+        PART[(NW + lw) * DE + q * 32 + lane] = ah[q];
+        v[1] = fma(yq[q], au[q], v[1]);
+        v[2] = fma(gxq[q], au[q], v[2]);
+        v[4] = fma(gxq[q], ah[q], v[4]);
+        if (lw == 0) {
+          v[0] = fma(sq[q], yq[q], v[0]);
+          v[3] = fma(sq[q], gxq[q], v[3]);
+          v[5] = fma(gxq[q], gxq[q], v[5]);
+        }
+      }
+      v[6] = (double)stop_seen;
+      stop_seen = stop_now;
+      grp.template sum<7>(v); // its barrier also publishes the partials
+      const bool skipped = fabs(v[0]) < kMinCurvature;
+      const double sg = v[3], gh = v[4];
+      double rho = 0.0, hb = 0.0, wg = 0.0;
+      if (!skipped) {
+        rho = 1.0 / v[0];
+        hb = 0.5 * rho * fma(rho, v[1], 1.0);
+        wg = hb * sg - rho * v[2];
+      }
+      if (owner) {
+        double u2[2] = {PART[t], NW > 1 ? PART[DE + t] : 0.0};
+        double h2[2] = {PART[NW * DE + t], NW > 1 ? PART[(NW + 1) * DE + t] : 0.0};
+#pragma unroll
+        for (int w = 2; w < NW; ++w) {
+          u2[w & 1] += PART[w * DE + t];
+          h2[w & 1] += PART[(NW + w) * DE + t];
+        }
+        const double uu = u2[0] + u2[1], hh = h2[0] + h2[1];
+        double s_r = sq[0];
+#pragma unroll
+        for (int q = 1; q < R; ++q)
+          if (q == lw)
+            s_r = sq[q];
+        double pn;
+        if (!skipped) {
+          const double wi = fma(hb, s_r, -rho * uu);
+          pn = -(hh + s_r * wg + wi * sg);
+          *reinterpret_cast<double2*>(SW + 2 * t) = make_double2(s_r, wi);
+        } else {
+          pn = -hh;
+        }
+        XP[t] = make_double2(take ? fma(alpha, xpo.y, xpo.x) : xpo.x, pn);
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q)
+        gq[q] = gxq[q];
+      pend = !skipped;
+      ddir = skipped ? -gh : -(gh + 2.0 * sg * wg);
+      stop = v[6] != 0.0;
+      if (take)
+        best = fnew;
+      // ||g|| = sqrt(g.g): taken only where it decides something (far
+      // above tol^2, g.g cannot pass the test)
+      if (!isfinite(v[5]) || !isfinite(fnew)) {
+        status = kNonFinite;
+        fout = fnew;
+        gout = sqrt(v[5]);
+        break;
+      }
+      if (v[5] <= tol_sq4 && sqrt(v[5]) < prm.tol) {
+        if (t == 0)
+          note_converged(ctl, prm.required);
+        status = kConverged;
+        fout = best;
+        gout = sqrt(v[5]);
+        break;
+      }
+      if (!take && skipped && !(prm.flags & kFlagNoFixedPoint)) {
+        executed = iter + 1;
+        iter = prm.max_iter;
+        break;
+      }
+      grp.sync(); // {x, p} and {s, w} written before the next line search
+    }
+    if (status == kUnset || status == kStopped) {
+      if (status == kUnset)
+        status = kSurrender;
+      fout = best;
+      double gg[1] = {0.0};
+      if (lw == 0) {
+#pragma unroll
+        for (int q = 0; q < R; ++q)
+          gg[0] = fma(gq[q], gq[q], gg[0]);
+      }
+      grp.template sum<1, 1>(gg);
+      gout = sqrt(gg[0]);
+    }
+    if (owner && out.x)
+      out.x[run * D + r] = XP[t].x;
+    if (t == 0) {
+      if (out.fval)
+        out.fval[run] = fout;
+      if (out.status)
+        out.status[run] = status;
+      if (out.iter)
+        out.iter[run] = iter;
+      if (out.gnorm)
+        out.gnorm[run] = gout;
+      if (out.counters) {
+        out.counters[3 * run + 0] = executed >= 0 ? executed : iter;
+        out.counters[3 * run + 1] = n_eval;
+        out.counters[3 * run + 2] = n_grad;
+      }
+    }
+    grp.sync(); // the group's shared memory is free for its next run
+  }
+
+  // One run on the group: the line form where the objective has one,
+  // gradients are analytic and a lane holds at most two rows, else trial
+  // points in shared memory.  (At D = 128, four rows a lane on twelve
+  // warps, the line form measured slower on a B200: twelve warps each
+  // computing all 128 gradient entries and a twelve-warp reduction cost
+  // more than the two barriers saved.)
+  inline constexpr int kRowLineMaxDim = 64;
+
+  template <class F, int D, int NW, bool Adjoint>
+  __device__ __forceinline__ void
+  row_run(const F& f, double* sm, int bar, int base, const BfgsParams& prm,
+          const double* __restrict__ x0, int64_t run, const RunOut& out,
+          Control* ctl)
+  {
+    if constexpr (Adjoint && RowLineObjective<F> && D <= kRowLineMaxDim)
+      row_run_line<F, D, NW>(f, sm, bar, base, prm, x0, run, out, ctl);
+    else
+      row_run_points<F, D, NW, Adjoint>(f, sm, bar, base, prm, x0, run, out, ctl);
   }
 
   // Warps of a group for D in a block of `block` threads: among the counts

@@ -196,6 +196,57 @@ namespace zeus {
         g[i] = gi;
       });
     }
+
+    // Line forms: coordinate i of x + a p is fma(a, p_i, x_i), read from
+    // {x_i, p_i} pairs stored at slot (i % R) * 32 + i / R (D = 32 R; R = 1
+    // is natural order), so trial points need not be stored.  Member m of
+    // an S-lane group takes the terms whose first coordinate sits at slots
+    // m, m + S, ...: consecutive members read consecutive slots for both of
+    // a term's coordinates.  Two accumulators, as in value_coop.
+    template <int S, int R>
+    __device__ __forceinline__ double
+    value_line_part(const double2* xp, double a, int m) const
+    {
+      static_assert((int)D == 32 * R, "one slot per lane and row");
+      double acc[2] = {0.0, 0.0};
+#pragma unroll
+      for (int k = 0; k < ((int)D + S - 1) / S; ++k) {
+        const int p = m + k * S;
+        const int i = (p % 32) * R + p / 32;
+        if (p < (int)D && i < (int)D - 1) {
+          const int pn = R == 1 ? p + 1 : p / 32 < R - 1 ? p + 32 : p % 32 + 1;
+          const double2 u = xp[p], w = xp[pn];
+          const double xi = fma(a, u.y, u.x), xj = fma(a, w.y, w.x);
+          const double t1 = 1.0 - xi;
+          const double t2 = fma(-xi, xi, xj);
+          acc[k & 1] = fma(100.0 * t2, t2, fma(t1, t1, acc[k & 1]));
+        }
+      }
+      return acc[0] + acc[1];
+    }
+    // d/dx_i at x + a p, same storage (explicit FMAs: every call site
+    // rounds alike)
+    template <int R>
+    __device__ __forceinline__ double
+    gradient_line_entry(const double2* xp, double a, int i) const
+    {
+      const auto slot = [](int j) { return (j % R) * 32 + j / R; };
+      const double2 c = xp[slot(i)];
+      const double xi = fma(a, c.y, c.x);
+      double gi = 0.0;
+      if (i + 1 < (int)D) {
+        const double2 n = xp[slot(i + 1)];
+        const double t1 = 1.0 - xi;
+        const double t2 = fma(-xi, xi, fma(a, n.y, n.x));
+        gi = fma(-400.0 * xi, t2, -2.0 * t1);
+      }
+      if (i > 0) {
+        const double2 q = xp[slot(i - 1)];
+        const double xh = fma(a, q.y, q.x);
+        gi = fma(200.0, fma(-xh, xh, xi), gi);
+      }
+      return gi;
+    }
   };
 
   template <std::size_t D>
