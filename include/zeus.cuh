@@ -193,6 +193,22 @@ namespace zeus {
       return e;
     }
 
+    // The reference's per-timer report lines (bfgs_sequential.cuh:345-360),
+    // from zeus_cycle_metrics' values.
+    inline void
+    print_metrics(const char* label, float ms_opt, const double m[8])
+    {
+      std::printf("[%s] Kernel wall time: %.3f ms\n", label, ms_opt);
+      std::printf("[%s] Avg cycles/thread: %.3f ; avg ms/thread: %.6f\n", label, m[6],
+                  m[7]);
+      std::printf("[%s] Calls/thread \u2248 %.2f; ms/call \u2248 %.6f\n", label, m[1],
+                  m[0]);
+      std::printf("[%s] Heuristic fraction: %.3f%%\n", label, 100.0 * m[5]);
+      std::printf("[%s] Serialized sum: %.3f ms; fraction vs kernel: %.3f%%\n", label,
+                  m[4] * ms_opt, 100.0 * m[4]);
+      std::printf("[%s] Block-level fraction p95: %.3f%%\n", label, 100.0 * m[3]);
+    }
+
     // hws: for the CTA layout past about D = 160, a device buffer of
     // cta_h_slices(n) * D * D doubles holding each block's H
     inline int64_t
@@ -213,21 +229,21 @@ namespace zeus {
       constexpr bool kAdj = zb::HasAdjoint<F>;
       if constexpr (D <= 8) {
         const unsigned grid = (unsigned)((prm.n + 127) / 128);
-        zb::bfgs_thread_kernel<F, (int)D, kAdj>
+        zb::bfgs_thread_kernel<F, (int)D, kAdj, true>
           <<<grid, 128, 0, st>>>(f, prm, starts, out, ctl);
       } else if constexpr (D <= 32) {
         constexpr int TS = 32, TPB = zb::kTileBlock / TS;
         const unsigned grid = (unsigned)((prm.n + TPB - 1) / TPB);
         const size_t smem =
           sizeof(double) * TPB * zb::tile_smem_doubles<(int)D, TS>();
-        zb::bfgs_tile_kernel<F, (int)D, TS, kAdj>
+        zb::bfgs_tile_kernel<F, (int)D, TS, kAdj, true>
           <<<grid, zb::kTileBlock, smem, st>>>(f, prm, starts, out, ctl);
       } else {
         static_assert(D <= 1024, "dimensions above 1024 are not supported");
         constexpr int B = D <= 64 ? 256 : 512;
         const size_t smem =
           sizeof(double) * zb::cta_smem_doubles<F, (int)D, kAdj>(B);
-        auto k = zb::bfgs_cta_kernel<F, (int)D, kAdj, B>;
+        auto k = zb::bfgs_cta_kernel<F, (int)D, kAdj, B, true>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
         int dev = 0, sms = 0, per_sm = 0;
@@ -324,8 +340,12 @@ namespace zeus {
         throw cudaErrorLaunchFailure;
       }
       zb::BfgsParams prm{n, MAX_ITER, requiredConverged, tolerance, 0};
+      // per-run counters and the AD / BFGS / total cycle timers of the
+      // reference's metrics (bfgs_sequential.cuh:447-470)
+      int64_t* counters = b.alloc<int64_t>(N * 3);
+      int64_t* cycles = b.alloc<int64_t>(N * 3);
       zb::RunOut out{fval,   status,  iter,    gnorm,   x,
-                     nullptr, nullptr, nullptr, nullptr, nullptr};
+                     counters, nullptr, nullptr, nullptr, nullptr, cycles};
       const bool traj = !trajectory_file.empty() && MAX_ITER > 0;
       const size_t steps = traj ? (size_t)N * (size_t)MAX_ITER : 0;
       if (traj) {
@@ -397,6 +417,27 @@ namespace zeus {
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
       best.ms_opt = ms;
+      double met[2][8] = {};
+      {
+        std::vector<int64_t> hcy((size_t)N * 3), hct((size_t)N * 3);
+        cudaMemcpy(hcy.data(), cycles, hcy.size() * sizeof(int64_t),
+                   cudaMemcpyDeviceToHost);
+        cudaMemcpy(hct.data(), counters, hct.size() * sizeof(int64_t),
+                   cudaMemcpyDeviceToHost);
+        int dev = 0, khz = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dev);
+        const char* label[2] = {"AD", "BFGS"};
+        Metrics* dst[2] = {&best.ad, &best.bfgs};
+        for (int w = 0; w < 2; ++w) {
+          if (zeus_cycle_metrics(hcy.data(), hct.data(), n, w, (double)khz, ms,
+                                 128, met[w]) != ZEUS_OK)
+            continue;
+          detail::print_metrics(label[w], ms, met[w]);
+          *dst[w] = Metrics{label[w], met[w][0], met[w][1], met[w][5],
+                            met[w][3], met[w][4], met[w][2]};
+        }
+      }
       best.c = Convergence{hc.actual, hc.claimed, hc.surrendered, hc.stopped};
       if (hc.best_idx >= 0) {
         const int i = hc.best_idx;
@@ -422,9 +463,12 @@ namespace zeus {
                            best.iter, 0};
       const zeus_census zc{hc.actual, hc.claimed, hc.surrendered, hc.stopped,
                            hc.best_idx, 0};
+      const double tsv_metrics[10] = {met[0][0], met[0][1], met[0][2], met[0][3],
+                                      met[0][4], met[1][0], met[1][1], met[1][2],
+                                      met[1][3], met[1][4]};
       if (zeus_append_results_tsv(nullptr, fn.c_str(), run, n, (int32_t)D, ms_init,
                                   ms_pso, ms, 0.f, MAX_ITER, PSO_ITER, err, &zr, &zc,
-                                  best.coordinates, nullptr) != ZEUS_OK)
+                                  best.coordinates, tsv_metrics) != ZEUS_OK)
         std::fprintf(stderr, "Error: %s\n", zeus_last_error());
       std::printf("claimed: %d\tactual : %d\tsurrendered: %d\tstopped: %d\n",
                   hc.claimed, hc.actual, hc.surrendered, hc.stopped);

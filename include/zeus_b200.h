@@ -112,7 +112,16 @@ typedef struct zeus_bfgs_config {
  * {BFGS iterations, f evaluations, gradient evaluations} as int64[3].
  * Trajectories use the reference layout [iter][dim][run] and [iter][run]
  * (bfgs_sequential.cuh:100-109); they must hold max_iter steps and be
- * prefilled by the caller (NaN, status -1). */
+ * prefilled by the caller (NaN, status -1).  cycles (optional) receives per
+ * run {gradient cycles, update cycles, whole-run cycles} as int64[3]: the
+ * reference's ad_cycles / bfgs_cycles / total_cycles clock64 timers
+ * (bfgs_sequential.cuh:40-44, 222-232), sampled only when it is non-NULL.
+ * The update span includes the new search direction where a layout forms
+ * both in one pass over H.  Calls per run follow from counters' gradient
+ * evaluations (see zeus_cycle_metrics).  zeus_bfgs_device samples them
+ * (its kernels are built with and without the timers, so asking costs
+ * nothing when not asked); the persistent batch does not and rejects a class
+ * whose cycles are set. */
 typedef struct zeus_run_outputs {
   double* fval;
   int32_t* status;
@@ -124,6 +133,7 @@ typedef struct zeus_run_outputs {
   double* traj_f;
   double* traj_g;
   int8_t* traj_status;
+  int64_t* cycles;
 } zeus_run_outputs;
 
 /* The reference's Result<D> minus the coordinate array (util.hpp:36-54). */
@@ -464,14 +474,32 @@ double zeus_euclidean_error(const char* fun_name, const double* x, int32_t dim);
  * as %e; `time` is ms_init + ms_pso + ms_opt + ms_rand when pso_iter > 0,
  * else ms_opt + ms_rand.  `metrics` holds the AD then BFGS
  * {ms_per_call, calls_per_thread_mean, fraction_of_thread, block95,
- * serialized} (10 doubles) or NULL for zeros: this library does not sample
- * per-call cycle counts. */
+ * serialized} (10 doubles, see zeus_cycle_metrics) or NULL for zeros. */
 int zeus_append_results_tsv(const char* dir, const char* fun_name, int32_t run,
                             int64_t n, int32_t dim, float ms_init, float ms_pso,
                             float ms_opt, float ms_rand, int32_t max_iter,
                             int32_t pso_iter, double error,
                             const zeus_result* best, const zeus_census* census,
                             const double* coords, const double* metrics);
+
+/* Replaces bfgs::sequential::report_metrics_and_cleanup
+ * (bfgs_sequential.cuh:236-373) for one of its two timers, from HOST
+ * copies of zeus_run_outputs' cycles and counters (n runs each): `which` 0
+ * is the AD timer (gradient cycles; calls = gradient evaluations), 1 the
+ * BFGS timer (update cycles; calls = updates, one after every gradient
+ * evaluation but the first).  With the SM clock in kHz (the
+ * device's clockRate, which the reference uses) and the launch's ms_opt,
+ * fills by the reference's formulas, a run standing for its thread,
+ * metrics[8] = {ms_per_call, calls_per_thread_mean, fraction_of_thread,
+ * block95, serialized (the results file's five, in its order),
+ * fraction_of_kernel, avg_cycles_per_thread, avg_ms_per_thread}:
+ * fraction_of_thread is the mean of cycles / whole-run cycles, block95 the
+ * 95th percentile over consecutive groups of `runs_per_block` runs of their
+ * summed time / ms_opt, serialized the summed time / ms_opt.  Does not
+ * print. */
+int zeus_cycle_metrics(const int64_t* cycles, const int64_t* counters, int64_t n,
+                       int32_t which, double sm_clock_khz, float ms_opt,
+                       int32_t runs_per_block, double metrics[8]);
 
 /* ---- measurement ----------------------------------------------------
  * No counterpart in the reference: a roofline probe.  Runs `iters`

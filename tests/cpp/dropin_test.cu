@@ -86,9 +86,14 @@ emit(const char* name, const zeus::Result<D>& r)
 {
   std::printf("{\"case\": \"%s\", \"status\": %d, \"fval\": %.17g, \"gnorm\": %.17g, "
               "\"iter\": %d, \"idx\": %d, \"claimed\": %d, \"stopped\": %d, "
-              "\"surrendered\": %d, \"x\": [",
+              "\"surrendered\": %d, \"ad\": [%.17g, %.17g, %.17g, %.17g, %.17g, %.17g], "
+              "\"bfgs\": [%.17g, %.17g, %.17g, %.17g, %.17g, %.17g], \"x\": [",
               name, r.status, r.fval, r.gradientNorm, r.iter, r.idx, r.c.claimed,
-              r.c.stopped, r.c.surrendered);
+              r.c.stopped, r.c.surrendered, r.ad.ms_per_call, r.ad.calls_per_thread_mean,
+              r.ad.fraction_of_kernel, r.ad.block95, r.ad.serialized,
+              r.ad.fraction_of_thread, r.bfgs.ms_per_call, r.bfgs.calls_per_thread_mean,
+              r.bfgs.fraction_of_kernel, r.bfgs.block95, r.bfgs.serialized,
+              r.bfgs.fraction_of_thread);
   for (std::size_t i = 0; i < D; ++i)
     std::printf("%s%.17g", i ? ", " : "", r.coordinates[i]);
   std::printf("]}\n");

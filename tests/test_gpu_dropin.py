@@ -128,6 +128,32 @@ def test_results_files_like_the_reference(results, workdir):
         assert (workdir / f"zeus_{d}d_results.tsv").exists()
 
 
+def test_cycle_metrics_like_the_reference(results, workdir):
+    """Every call samples the reference's AD / BFGS / total cycle timers
+    (bfgs_sequential.cuh:93-97, 150-174, 229-232) and reports their summary
+    (report_metrics_and_cleanup, :236-373) in Result::ad / ::bfgs and in the
+    results row's ten metric columns."""
+    for case in ("rosenbrock", "sphere16", "gaussian8", "sphere40", "sphere200", "traj"):
+        r = results[case]
+        ad, bf = r["ad"], r["bfgs"]  # ms/call, calls, kernel frac, p95, serialized, thread frac
+        assert ad[0] > 0 and bf[0] > 0, case
+        assert ad[1] >= 1.0 and bf[1] >= 0.0, case  # the first gradient counts
+        assert ad[1] == pytest.approx(bf[1] + 1.0, abs=1e-9), case
+        for m in (ad, bf):
+            assert 0.0 < m[5] < 1.0 and m[2] > 0 and m[3] > 0 and m[4] > 0, (case, m)
+        assert ad[5] + bf[5] < 1.0, case  # parts of the run
+    rows = (workdir / "zeus_2d_results.tsv").read_text().splitlines()
+    f = rows[1].split("\t")
+    ad = [float(v) for v in f[4:9]]
+    bf = [float(v) for v in f[9:14]]
+    r = results["rosenbrock"]
+    # file order: ms_per_call, calls_per_thread_mean, fraction_of_thread, block95, serialized
+    assert ad[0] == pytest.approx(r["ad"][0], rel=1e-5)
+    assert ad[1] == pytest.approx(r["ad"][1], rel=1e-5)
+    assert ad[2] == pytest.approx(r["ad"][5], rel=1e-5)
+    assert bf[4] == pytest.approx(r["bfgs"][4], rel=1e-5)
+
+
 def test_cta_layout_with_h_in_global_memory(results):
     """D = 200: H (320 KB) does not fit in shared memory; each block streams
     its own slice of a global workspace."""

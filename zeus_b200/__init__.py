@@ -107,6 +107,7 @@ class RunOutputs(C.Structure):
         ("traj_f", C.c_void_p),
         ("traj_g", C.c_void_p),
         ("traj_status", C.c_void_p),
+        ("cycles", C.c_void_p),
     ]
 
 
@@ -240,6 +241,8 @@ SIGNATURES = {
         C.c_int, [C.c_char_p, C.c_char_p, C.c_int32, C.c_int64, C.c_int32, C.c_float,
                   C.c_float, C.c_float, C.c_float, C.c_int32, C.c_int32, C.c_double,
                   C.POINTER(CResult), C.POINTER(CCensus), _P, _P]),
+    "zeus_cycle_metrics": (
+        C.c_int, [_P, _P, C.c_int64, C.c_int32, C.c_double, C.c_float, C.c_int32, _P]),
     "zeus_autotune": (
         C.c_int,
         [C.POINTER(Problem), C.POINTER(BfgsConfig), C.c_int64, C.c_uint64, C.c_double,

@@ -170,6 +170,11 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
       set_error("zeus_batch_device: class %d is invalid or not built", i);
       return ZEUS_E_INVALID;
     }
+    if (c.out.cycles) {
+      set_error("zeus_batch_device: class %d asks for cycles, which the batch kernel "
+                "does not sample (zeus_bfgs_device does)", i);
+      return ZEUS_E_UNSUPPORTED;
+    }
     int layout = c.layout, tile = c.tile;
     if (layout == ZEUS_LAYOUT_AUTO)
       batch_default(p.kind, p.dim, config->gradient, &layout, &tile);
@@ -187,7 +192,7 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
     b.starts = c.d_starts;
     b.out = RunOut{c.out.fval,   c.out.status, c.out.iter,   c.out.gnorm,
                    c.out.x,      c.out.counters, nullptr,     nullptr,
-                   nullptr,      nullptr};
+                   nullptr,      nullptr,        nullptr};
     b.ctl = reinterpret_cast<Control*>(c.d_control);
     b.data = p.data;
     b.idata = p.idata;

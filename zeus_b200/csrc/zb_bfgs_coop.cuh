@@ -140,7 +140,7 @@ namespace zb {
   // forms u = H y and h = H g_next together, and one butterfly reduction of
   // {s.y, y.u, u.g, s.g, g.h, g.g, stop} gives every scalar:
   //   p+ = -(h + s (w.g) + w (s.g)),  g.p+ = -(g.h + 2 (s.g)(w.g)).
-  template <class F, int D, int TS, bool Adjoint>
+  template <class F, int D, int TS, bool Adjoint, bool kTimed = false>
   __device__ __forceinline__ void
   tile_run(const F& f, cg::thread_block_tile<TS> tile, double* buf,
            const BfgsParams& prm, const double* __restrict__ x0, int64_t run,
@@ -170,9 +170,12 @@ namespace zb {
         H[r][j] = (i == j) ? 1.0 : 0.0;
     }
     grp.sync();
+    const CycleTimer<kTimed> tm(out, run, lane == 0);
     double best = coop_value<F, D>(f, grp, xs);
+    tm.start_grad();
     coop_gradient_only<F, D, Adjoint>(f, grp, xs, gs);
     grp.sync();
+    tm.stop_grad();
     double ddir;
     bool stop;
     {
@@ -287,9 +290,11 @@ namespace zb {
           xs[i] = xn[r];
       }
       grp.sync();
+      tm.start_grad();
       coop_gradient_only<F, D, Adjoint>(f, grp, xs, gs);
       ++n_grad;
       grp.sync();
+      tm.stop_grad();
       const bool take = fnew < best;
       double gn[R], s[R], y[R], gx[R];
 #pragma unroll
@@ -305,6 +310,7 @@ namespace zb {
       grp.sync();
       // ---- one pass: deferred update, u = H y, h = H g_next (even and odd
       // columns in separate sums: half the chain of dependent FMAs)
+      tm.start_update();
       double u[R], hh[R];
       {
         double ua[R][2], ha[R][2];
@@ -378,6 +384,7 @@ namespace zb {
           p[r] = -hh[r];
         }
       }
+      tm.stop_update();
       pend = !skipped;
       ddir = skipped ? -gh : -(gh + 2.0 * sg * wg);
       stop = v[6] != 0.0;
@@ -440,11 +447,12 @@ namespace zb {
         out.counters[3 * run + 1] = n_eval;
         out.counters[3 * run + 2] = n_grad;
       }
+      tm.finish();
     }
     grp.sync();
   }
 
-  template <class F, int D, int TS, bool Adjoint>
+  template <class F, int D, int TS, bool Adjoint, bool kTimed = false>
   __global__ void __launch_bounds__(kTileBlock)
     bfgs_tile_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
                      RunOut out, Control* ctl)
@@ -456,8 +464,8 @@ namespace zb {
     const int64_t run = (int64_t)blockIdx.x * TPB + tslot;
     if (run >= prm.n)
       return; // the whole tile leaves together
-    tile_run<F, D, TS, Adjoint>(f, tile, sm + tslot * tile_smem_doubles<D, TS>(),
-                                prm, starts + run * D, run, out, ctl);
+    tile_run<F, D, TS, Adjoint, kTimed>(f, tile, sm + tslot * tile_smem_doubles<D, TS>(),
+                                        prm, starts + run * D, run, out, ctl);
   }
 
   // ---------------------------------------------------------------- CTA
@@ -625,7 +633,7 @@ namespace zb {
   // One run on the whole block (blockDim.x == kBlock): `sm` holds
   // cta_smem_doubles<F, D, Adjoint>(kBlock) doubles, 16-byte aligned; start
   // x0[D]; results to slot `run`.
-  template <class F, int D, bool Adjoint, int kBlock>
+  template <class F, int D, bool Adjoint, int kBlock, bool kTimed = false>
   __device__ __forceinline__ void
   cta_run(const F& f, double* sm, const BfgsParams& prm,
           const double* __restrict__ x0, int64_t run, const RunOut& out,
@@ -699,7 +707,9 @@ namespace zb {
       xcur[i] = x0[i];
     __syncthreads();
     int cur = 0; // current gradient in slot cur, the new one goes to cur ^ 1
+    const CycleTimer<kTimed> tm(out, run, t == 0);
     double best;
+    tm.start_grad();
     if constexpr (kTrialGrad)
       best = coop_gradient<F, D, Adjoint>(f, grp, xt, gb);
     else {
@@ -707,6 +717,7 @@ namespace zb {
       coop_gradient_only<F, D, Adjoint>(f, grp, xt, gb);
     }
     __syncthreads();
+    tm.stop_grad();
     double ddir;
     bool stop;
     {
@@ -934,15 +945,18 @@ namespace zb {
         xnr[r] = fma(alpha, pr[r], xr[r]);
       double* gn = gb + (cur ^ 1) * D;
       const double* g = gb + cur * D;
+      tm.start_grad();
       if constexpr (!kTrialGrad)
         coop_gradient_only<F, D, Adjoint>(f, grp, xn_s, gn);
       ++n_grad;
       __syncthreads();
+      tm.stop_grad();
       const bool take = fnew < best;
       const double* gx = take ? gn : g; // the gradient p+ is formed for
 
       // ---- sweep: deferred update + column sums of H y and H g_next, and
       // the seven values of the iteration's one reduction
+      tm.start_update();
       double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
       if constexpr (kColWarp) {
         if (warp < D / 8) {
@@ -1123,6 +1137,7 @@ namespace zb {
             xcur[i] = xnr[r];
         }
       }
+      tm.stop_update();
       pend = !skipped;
       ddir = skipped ? -gh : -(gh + 2.0 * sg * wg);
       stop = v[6] != 0.0;
@@ -1195,6 +1210,7 @@ namespace zb {
         out.counters[3 * run + 1] = n_eval;
         out.counters[3 * run + 2] = n_grad;
       }
+      tm.finish();
     }
     __syncthreads();
   }
@@ -1204,7 +1220,7 @@ namespace zb {
   // then takes runs gridDim.x, gridDim.x + 1, ... from the counter as it
   // finishes them, so a long run does not hold back runs statically queued
   // behind it; without a queue, block b runs b, b + gridDim.x, ...
-  template <class F, int D, bool Adjoint, int kBlock>
+  template <class F, int D, bool Adjoint, int kBlock, bool kTimed = false>
   __global__ void __launch_bounds__(kBlock)
     bfgs_cta_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
                     RunOut out, Control* ctl, double* __restrict__ hws = nullptr,
@@ -1214,8 +1230,8 @@ namespace zb {
     double* hg = hws ? hws + (size_t)blockIdx.x * D * D : nullptr;
     int64_t run = blockIdx.x;
     while (run < prm.n) {
-      cta_run<F, D, Adjoint, kBlock>(f, sm, prm, starts + run * D, run, out,
-                                     ctl, hg);
+      cta_run<F, D, Adjoint, kBlock, kTimed>(f, sm, prm, starts + run * D, run, out,
+                                             ctl, hg);
       if (!queue) {
         run += gridDim.x;
         continue;

@@ -90,15 +90,18 @@ namespace zb {
         H[e] = (e / D == e % D) ? 1.0 : 0.0;
       long long n_eval = 0, n_grad = 0;
       __syncthreads();
+      const CycleTimer<true> tm(out, idx, tid == 0);
       if (tid == 0) {
         sh.best = eval_array<F, D>(f, x);
         sh.done = 0;
         sh.status = kUnset;
       }
+      tm.start_grad();
       exact_dual_gradient<F, D>(f, x, g);
       ++n_eval;
       ++n_grad;
       __syncthreads();
+      tm.stop_grad();
 
       int iter;
       for (iter = 0; iter < prm.max_iter; ++iter) {
@@ -189,9 +192,11 @@ namespace zb {
             ++n_eval;
           }
         }
+        tm.start_grad();
         exact_dual_gradient<F, D>(f, xn, gn);
         ++n_grad;
         __syncthreads();
+        tm.stop_grad();
         for (int i = tid; i < D; i += bs)
           y[i] = gn[i] - g[i];
         __syncthreads();
@@ -202,6 +207,7 @@ namespace zb {
           sh.sy = sy;
         }
         __syncthreads();
+        tm.start_update();
         if (!(::fabs(sh.sy) < kMinCurvature)) {
           const double rho = 1.0 / sh.sy;
           for (int e = tid; e < D * D; e += bs) {
@@ -226,6 +232,7 @@ namespace zb {
         }
         const bool skipped = ::fabs(sh.sy) < kMinCurvature;
         __syncthreads();
+        tm.stop_update();
         const bool take = sh.fnew < sh.best;
         if (take)
           for (int i = tid; i < D; i += bs) {
@@ -293,6 +300,7 @@ namespace zb {
           out.counters[3 * (size_t)idx + 1] = n_eval;
           out.counters[3 * (size_t)idx + 2] = n_grad;
         }
+        tm.finish();
       }
       if (out.x)
         for (int d = tid; d < D; d += bs)

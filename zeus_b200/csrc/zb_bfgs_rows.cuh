@@ -157,7 +157,7 @@ namespace zb {
   // row_smem_doubles<D, NW>() doubles (16-byte aligned); the group is
   // threads [base, base + 32 NW) of the block, synchronised by named
   // barrier `bar`.
-  template <class F, int D, int NW, bool Adjoint>
+  template <class F, int D, int NW, bool Adjoint, bool kTimed = false>
   __device__ __forceinline__ void
   row_run_points(const F& f, double* sm, int bar, int base, const BfgsParams& prm,
                  const double* __restrict__ x0, int64_t run, const RunOut& out,
@@ -195,9 +195,12 @@ namespace zb {
     for (int i = t; i < D; i += NT)
       X[i] = x0[i];
     grp.sync();
+    const CycleTimer<kTimed> tm(out, run, t == 0);
     double best = coop_value<F, D>(f, grp, X);
+    tm.start_grad();
     coop_gradient_only<F, D, Adjoint>(f, grp, X, G);
     grp.sync();
+    tm.stop_grad();
     double ddir;
     bool stop;
     {
@@ -282,12 +285,14 @@ namespace zb {
       const double* xa = TX + found * TSTR; // the accepted point
       double* gn = G + (cur ^ 1) * DE;
       const double* g = G + cur * DE;
+      tm.start_grad();
       {
         const OwnerGroup<NT, R> og{grp};
         coop_gradient_only<F, D, Adjoint>(f, og, xa, gn);
         if constexpr (!OwnerWritesGradient<F, OwnerGroup<NT, R>, Adjoint>)
           grp.sync();
       }
+      tm.stop_grad();
       ++n_grad;
       const bool take = fnew < best;
       double s_r = 0.0, y_r = 0.0, gx_r = 0.0;
@@ -302,6 +307,7 @@ namespace zb {
 
       // ---- the pass over H: deferred update, partial sums of H y and H g_x
       // over this warp's columns for this lane's rows
+      tm.start_update();
       double au[R], ah[R];
 #pragma unroll
       for (int q = 0; q < R; ++q) {
@@ -395,6 +401,7 @@ namespace zb {
         if (take)
           X[r] = xa[r];
       }
+      tm.stop_update();
       pend = !skipped;
       ddir = skipped ? -gh : -(gh + 2.0 * sg * wg);
       stop = v[6] != 0.0;
@@ -453,6 +460,7 @@ namespace zb {
         out.counters[3 * run + 1] = n_eval;
         out.counters[3 * run + 2] = n_grad;
       }
+      tm.finish();
     }
     grp.sync(); // the group's shared memory is free for its next run
   }
@@ -500,7 +508,7 @@ namespace zb {
   //      iteration barrier publishes them.
   // The arithmetic of a run is that of row_run_points up to the order of
   // the reductions' additions.
-  template <class F, int D, int NW>
+  template <class F, int D, int NW, bool kTimed = false>
   __device__ __forceinline__ void
   row_run_line(const F& f, double* sm, int bar, int base, const BfgsParams& prm,
                const double* __restrict__ x0, int64_t run, const RunOut& out,
@@ -537,9 +545,12 @@ namespace zb {
     for (int i = t; i < D; i += NT)
       X0[i] = x0[i];
     grp.sync();
+    const CycleTimer<kTimed> tm(out, run, t == 0);
     double best = coop_value<F, D>(f, grp, X0);
+    tm.start_grad();
     coop_gradient_only<F, D, true>(f, grp, X0, G0);
     grp.sync();
+    tm.stop_grad();
     double gq[R]; // the gradient at x, this lane's rows
 #pragma unroll
     for (int q = 0; q < R; ++q)
@@ -606,6 +617,7 @@ namespace zb {
       ++n_grad;
       // ---- gradient entries at the accepted point for this lane's rows,
       // into the warp's {y, g_x} table
+      tm.start_grad();
       double sq[R], yq[R], gxq[R];
       double2 xpo = make_double2(0.0, 0.0); // the owner's {x, p}
       double* yg_w = YGW + 2 * D * lw;
@@ -621,6 +633,8 @@ namespace zb {
           xpo = c;
       }
       __syncwarp();
+      tm.stop_grad();
+      tm.start_update();
 
       // ---- the pass over H: deferred update, partial sums of H y and H g_x
       double au[R], ah[R];
@@ -716,6 +730,7 @@ namespace zb {
         }
         XP[t] = make_double2(take ? fma(alpha, xpo.y, xpo.x) : xpo.x, pn);
       }
+      tm.stop_update();
 #pragma unroll
       for (int q = 0; q < R; ++q)
         gq[q] = gxq[q];
@@ -776,6 +791,7 @@ namespace zb {
         out.counters[3 * run + 1] = n_eval;
         out.counters[3 * run + 2] = n_grad;
       }
+      tm.finish();
     }
     grp.sync(); // the group's shared memory is free for its next run
   }
@@ -788,16 +804,17 @@ namespace zb {
   // more than the two barriers saved.)
   inline constexpr int kRowLineMaxDim = 64;
 
-  template <class F, int D, int NW, bool Adjoint>
+  template <class F, int D, int NW, bool Adjoint, bool kTimed = false>
   __device__ __forceinline__ void
   row_run(const F& f, double* sm, int bar, int base, const BfgsParams& prm,
           const double* __restrict__ x0, int64_t run, const RunOut& out,
           Control* ctl)
   {
     if constexpr (Adjoint && RowLineObjective<F> && D <= kRowLineMaxDim)
-      row_run_line<F, D, NW>(f, sm, bar, base, prm, x0, run, out, ctl);
+      row_run_line<F, D, NW, kTimed>(f, sm, bar, base, prm, x0, run, out, ctl);
     else
-      row_run_points<F, D, NW, Adjoint>(f, sm, bar, base, prm, x0, run, out, ctl);
+      row_run_points<F, D, NW, Adjoint, kTimed>(f, sm, bar, base, prm, x0, run, out,
+                                                ctl);
   }
 
   // Warps of a group for D in a block of `block` threads: among the counts
@@ -832,7 +849,7 @@ namespace zb {
 
   // Standalone launches: one group per block, blocks take runs from the
   // workspace queue as they finish (block b starts with run b).
-  template <class F, int D, int NW, bool Adjoint>
+  template <class F, int D, int NW, bool Adjoint, bool kTimed = false>
   __global__ void __launch_bounds__(32 * NW)
     bfgs_rows_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
                      RunOut out, Control* ctl, unsigned long long* queue)
@@ -842,7 +859,7 @@ namespace zb {
     double* slot = sm + row_smem_doubles<D, NW>() - 2;
     int64_t run = blockIdx.x;
     while (run < prm.n) {
-      row_run<F, D, NW, Adjoint>(f, sm, 1, 0, prm, starts + run * D, run, out, ctl);
+      row_run<F, D, NW, Adjoint, kTimed>(f, sm, 1, 0, prm, starts + run * D, run, out, ctl);
       if (threadIdx.x == 0)
         reinterpret_cast<long long*>(slot)[0] =
           (long long)gridDim.x + (long long)atomicAdd(queue, 1ull);

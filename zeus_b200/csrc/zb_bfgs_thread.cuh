@@ -68,7 +68,7 @@ namespace zb {
   }
 
   // One run, start x0[D], results to slot idx of `out`.
-  template <class F, int D, bool Adjoint>
+  template <class F, int D, bool Adjoint, bool kTimed = false>
   __device__ __forceinline__ void
   thread_run(const F& f, const BfgsParams& prm, const double* __restrict__ x0,
              int64_t idx, const RunOut& out, Control* ctl)
@@ -84,8 +84,11 @@ namespace zb {
       for (int j = i; j < D; ++j)
         H[tri<D>(i, j)] = (i == j) ? 1.0 : 0.0;
 
+    const CycleTimer<kTimed> tm(out, idx, true);
     double best = fast_value<F, D>(f, x);
+    tm.start_grad();
     fast_gradient<F, D, Adjoint>(f, x, g);
+    tm.stop_grad();
     long long n_eval = 1, n_grad = 1;
 #pragma unroll
     for (int i = 0; i < D; ++i)
@@ -125,8 +128,11 @@ namespace zb {
         ++n_eval;
       }
       double gn[D], s[D], y[D];
+      tm.start_grad();
       fast_gradient<F, D, Adjoint>(f, xn, gn);
+      tm.stop_grad();
       ++n_grad;
+      tm.start_update();
       double sy = 0.0;
 #pragma unroll
       for (int i = 0; i < D; ++i) {
@@ -158,6 +164,7 @@ namespace zb {
           for (int j = i; j < D; ++j)
             H[tri<D>(i, j)] += s[i] * w[j] + w[i] * s[j];
       }
+      tm.stop_update();
       const bool take = fnew < best;
       if (take) {
         best = fnew;
@@ -226,16 +233,17 @@ namespace zb {
       out.counters[3 * idx + 1] = n_eval;
       out.counters[3 * idx + 2] = n_grad;
     }
+    tm.finish();
   }
 
-  template <class F, int D, bool Adjoint>
+  template <class F, int D, bool Adjoint, bool kTimed = false>
   __global__ void __launch_bounds__(128)
     bfgs_thread_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
                        RunOut out, Control* ctl)
   {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx < prm.n)
-      thread_run<F, D, Adjoint>(f, prm, starts + idx * D, idx, out, ctl);
+      thread_run<F, D, Adjoint, kTimed>(f, prm, starts + idx * D, idx, out, ctl);
   }
 
 } // namespace zb

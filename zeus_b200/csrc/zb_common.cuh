@@ -65,7 +65,85 @@ namespace zb {
     double* traj_f;
     double* traj_g;
     int8_t* traj_status;
+    int64_t* cycles; // [run][3]: gradient, update, whole-run clock64 cycles
   };
+
+  // Per-run cycle counts, the reference's AD / BFGS / total timers
+  // (bfgs_sequential.cuh:93-97, 150-155, 166-174, 229-232), sampled only
+  // when the caller asked for them (RunOut::cycles non-null): clock64 spans
+  // of the gradient evaluations, of the inverse-Hessian update (with the
+  // new search direction where a layout fuses the two) and of the whole
+  // run, as the leader of the run's group (its rank 0) sees them.  The
+  // spans accumulate in the run's three output slots themselves (minus the
+  // clock at a span's start, plus it at its end), so the timer holds no
+  // registers across the loop.  Kernels instantiate it only when the
+  // caller asks for cycles (CycleTimer<false> is empty): even off, the
+  // timer's branches and stores cost the fused layouts several percent.
+  template <bool On = true>
+  struct CycleTimer {
+    const RunOut& out;
+    int64_t run;
+    bool lead;
+    __device__ __forceinline__
+    CycleTimer(const RunOut& o, int64_t r, bool leader)
+      : out(o), run(r), lead(leader)
+    {
+      if (out.cycles && lead) {
+        out.cycles[3 * run + 0] = 0;
+        out.cycles[3 * run + 1] = 0;
+        out.cycles[3 * run + 2] = -(int64_t)clock64();
+      }
+    }
+    __device__ __forceinline__ void
+    start(int k) const
+    {
+      if (out.cycles && lead)
+        out.cycles[3 * run + k] -= (int64_t)clock64();
+    }
+    __device__ __forceinline__ void
+    stop(int k) const
+    {
+      if (out.cycles && lead)
+        out.cycles[3 * run + k] += (int64_t)clock64();
+    }
+    __device__ __forceinline__ void
+    start_grad() const
+    {
+      start(0);
+    }
+    __device__ __forceinline__ void
+    stop_grad() const
+    {
+      stop(0);
+    }
+    __device__ __forceinline__ void
+    start_update() const
+    {
+      start(1);
+    }
+    __device__ __forceinline__ void
+    stop_update() const
+    {
+      stop(1);
+    }
+    // the whole run's span; after the run's last timed phase
+    __device__ __forceinline__ void
+    finish() const
+    {
+      stop(2);
+    }
+  };
+  template <>
+  struct CycleTimer<false> {
+    __device__ __forceinline__ CycleTimer(const RunOut&, int64_t, bool) {}
+    __device__ __forceinline__ void start_grad() const {}
+    __device__ __forceinline__ void stop_grad() const {}
+    __device__ __forceinline__ void start_update() const {}
+    __device__ __forceinline__ void stop_update() const {}
+    __device__ __forceinline__ void finish() const {}
+  };
+
+
 
   // {stop flag, converged count}: the reference's BFGSContext
   // (context.hpp:7-10), device-global.

@@ -27,7 +27,7 @@ namespace zb {
       return n < cap ? n : cap;
     }
 
-    template <class F, int D, bool Adj>
+    template <class F, int D, bool Adj, bool kTimed>
     int
     launch_one(const F& f, const BfgsParams& prm, const double* starts,
                const RunOut& out, Control* ctl, void* ws, size_t ws_bytes,
@@ -35,7 +35,7 @@ namespace zb {
     {
       constexpr int B = cta_block<D>();
       const size_t smem = sizeof(double) * cta_smem_doubles<F, D, Adj>(B);
-      auto kern = bfgs_cta_kernel<F, D, Adj, B>;
+      auto kern = bfgs_cta_kernel<F, D, Adj, B, kTimed>;
       int rc = cuda_fail(cudaFuncSetAttribute(
                            kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem),
@@ -76,7 +76,7 @@ namespace zb {
     // the row layout standalone: one group per block
     constexpr int kRowBlockCap = 384;
 
-    template <class F, int D, bool Adj>
+    template <class F, int D, bool Adj, bool kTimed>
     int
     launch_rows_one(const F& f, const BfgsParams& prm, const double* starts,
                     const RunOut& out, Control* ctl, void* ws, size_t ws_bytes,
@@ -84,7 +84,7 @@ namespace zb {
     {
       constexpr int NW = row_warps(D, kRowBlockCap), NT = 32 * NW;
       const size_t smem = sizeof(double) * row_smem_doubles<D, NW>();
-      auto kern = bfgs_rows_kernel<F, D, NW, Adj>;
+      auto kern = bfgs_rows_kernel<F, D, NW, Adj, kTimed>;
       int rc = cuda_fail(cudaFuncSetAttribute(
                            kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem),
@@ -145,9 +145,19 @@ namespace zb {
       using F = decltype(f);
       constexpr int D = (int)F::arity;
       if constexpr (rows_built<F>()) {
+        // the cycle timers are compiled in only where they are asked for
+        const bool timed = out.cycles != nullptr;
+        if (adjoint && timed)
+          return launch_rows_one<F, D, true, true>(f, prm, starts, out, ctl, ws, ws_bytes,
+                                                   st);
         if (adjoint)
-          return launch_rows_one<F, D, true>(f, prm, starts, out, ctl, ws, ws_bytes, st);
-        return launch_rows_one<F, D, false>(f, prm, starts, out, ctl, ws, ws_bytes, st);
+          return launch_rows_one<F, D, true, false>(f, prm, starts, out, ctl, ws, ws_bytes,
+                                                    st);
+        if (timed)
+          return launch_rows_one<F, D, false, true>(f, prm, starts, out, ctl, ws,
+                                                    ws_bytes, st);
+        return launch_rows_one<F, D, false, false>(f, prm, starts, out, ctl, ws, ws_bytes,
+                                                   st);
       } else {
         set_error("row layout: kind %d dim %d not built", F::kind, D);
         return ZEUS_E_UNSUPPORTED;
@@ -191,9 +201,15 @@ namespace zb {
       if constexpr (D >= kMinCtaDim &&
                     sizeof(double) * cta_smem_doubles_rt(D, cta_block<D>(), true) <=
                       kSmemLimit) {
+        // the cycle timers are compiled in only where they are asked for
+        const bool timed = out.cycles != nullptr;
+        if (adjoint && timed)
+          return launch_one<F, D, true, true>(f, prm, starts, out, ctl, ws, ws_bytes, st);
         if (adjoint)
-          return launch_one<F, D, true>(f, prm, starts, out, ctl, ws, ws_bytes, st);
-        return launch_one<F, D, false>(f, prm, starts, out, ctl, ws, ws_bytes, st);
+          return launch_one<F, D, true, false>(f, prm, starts, out, ctl, ws, ws_bytes, st);
+        if (timed)
+          return launch_one<F, D, false, true>(f, prm, starts, out, ctl, ws, ws_bytes, st);
+        return launch_one<F, D, false, false>(f, prm, starts, out, ctl, ws, ws_bytes, st);
       } else {
         set_error("CTA layout: dim %d not built", D);
         return ZEUS_E_UNSUPPORTED;

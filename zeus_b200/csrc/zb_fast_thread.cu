@@ -27,8 +27,16 @@ namespace zb {
       if constexpr (D <= kMaxThreadDim) {
         const int block = c.block > 0 ? c.block : kThreadBlock;
         const unsigned grid = (unsigned)((prm.n + block - 1) / block);
-        if (adjoint)
+        // the cycle timers are compiled in only where they are asked for
+        const bool timed = out.cycles != nullptr;
+        if (adjoint && timed)
+          bfgs_thread_kernel<F, D, true, true>
+            <<<grid, block, 0, st>>>(f, prm, starts, out, ctl);
+        else if (adjoint)
           bfgs_thread_kernel<F, D, true>
+            <<<grid, block, 0, st>>>(f, prm, starts, out, ctl);
+        else if (timed)
+          bfgs_thread_kernel<F, D, false, true>
             <<<grid, block, 0, st>>>(f, prm, starts, out, ctl);
         else
           bfgs_thread_kernel<F, D, false>

@@ -14,8 +14,16 @@ namespace zb {
       constexpr int TPB = kTileBlock / TS;
       const unsigned grid = (unsigned)((prm.n + TPB - 1) / TPB);
       const size_t smem = sizeof(double) * TPB * tile_smem_doubles<D, TS>();
-      if (adjoint)
+      // the cycle timers are compiled in only where they are asked for
+      const bool timed = out.cycles != nullptr;
+      if (adjoint && timed)
+        bfgs_tile_kernel<F, D, TS, true, true>
+          <<<grid, kTileBlock, smem, st>>>(f, prm, starts, out, ctl);
+      else if (adjoint)
         bfgs_tile_kernel<F, D, TS, true>
+          <<<grid, kTileBlock, smem, st>>>(f, prm, starts, out, ctl);
+      else if (timed)
+        bfgs_tile_kernel<F, D, TS, false, true>
           <<<grid, kTileBlock, smem, st>>>(f, prm, starts, out, ctl);
       else
         bfgs_tile_kernel<F, D, TS, false>

@@ -569,7 +569,7 @@ zeus_bfgs_device(const zeus_problem* problem, const zeus_bfgs_config* config,
                  config->tolerance, config->flags};
   RunOut ro{out->fval,     out->status, out->iter,   out->gnorm,
             out->x,        out->counters, out->traj_x, out->traj_f,
-            out->traj_g,   out->traj_status};
+            out->traj_g,   out->traj_status, out->cycles};
   Control* ctl = reinterpret_cast<Control*>(d_control);
   if (config->mode == ZEUS_MODE_EXACT)
     return launch_exact(o, prm, d_starts, ro, ctl, ws, kws, st);

@@ -1,6 +1,7 @@
 // Trajectory files: the per-iteration records of exact-mode runs written in
 // the reference's tab-separated layout (util::writeTrajectoryDataTSV,
 // src/utils.cu:128-176).  Host code only.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -209,6 +210,68 @@ zeus_append_results_tsv(const char* dir, const char* fun_name, int32_t run,
     set_error("zeus_append_results_tsv: write to %s failed", path.c_str());
     return ZEUS_E_INVALID;
   }
+  return ZEUS_OK;
+}
+
+int
+zeus_cycle_metrics(const int64_t* cycles, const int64_t* counters, int64_t n,
+                   int32_t which, double sm_clock_khz, float ms_opt,
+                   int32_t runs_per_block, double metrics[8])
+{
+  if (!cycles || !counters || !metrics || n <= 0 || (which != 0 && which != 1) ||
+      !(sm_clock_khz > 0.0) || runs_per_block <= 0) {
+    set_error("zeus_cycle_metrics: cycles, counters, metrics, n > 0, which 0/1, "
+              "a clock and runs_per_block > 0 are required");
+    return ZEUS_E_INVALID;
+  }
+  // the timer's cycles and calls per run: AD = gradient evaluations, BFGS =
+  // updates (one after each gradient evaluation but the first)
+  const int cyc_col = which == 0 ? 0 : 1;
+  const double hz = sm_clock_khz * 1000.0;
+  unsigned long long sum_cycles = 0ULL;
+  long long sum_calls = 0LL;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t grads = counters[3 * i + 2];
+    sum_cycles += (unsigned long long)cycles[3 * i + cyc_col];
+    sum_calls += which == 0 ? grads : (grads > 0 ? grads - 1 : 0);
+  }
+  const double avg_cycles = double(sum_cycles) / double(n);
+  const double avg_calls = sum_calls > 0 ? double(sum_calls) / double(n) : 0.0;
+  const double avg_cycles_per_call = avg_calls > 0 ? avg_cycles / avg_calls : 0.0;
+  const double ms_per_call = avg_cycles_per_call / hz * 1e3;
+  const double serialized_ms = double(sum_cycles) / hz * 1e3;
+  const double serialized = ms_opt > 0.0 ? serialized_ms / ms_opt : 0.0;
+  // mean over runs of this timer's share of the run's cycles
+  long double acc = 0.0L;
+  long long cnt = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    const double tot = (double)cycles[3 * i + 2];
+    if (tot > 0.0) {
+      acc += (long double)((double)cycles[3 * i + cyc_col] / tot);
+      ++cnt;
+    }
+  }
+  const double frac_thread = cnt > 0 ? (double)(acc / (long double)cnt) : 0.0;
+  // 95th percentile of the per-block summed time over ms_opt
+  const int64_t blocks = (n + runs_per_block - 1) / runs_per_block;
+  std::vector<long double> bc((size_t)blocks, 0.0L);
+  for (int64_t i = 0; i < n; ++i)
+    bc[(size_t)(i / runs_per_block)] += (long double)cycles[3 * i + cyc_col];
+  std::vector<double> fb((size_t)blocks);
+  for (int64_t b = 0; b < blocks; ++b)
+    fb[(size_t)b] = (double)(bc[(size_t)b] / hz * 1e3L) / (double)ms_opt;
+  std::sort(fb.begin(), fb.end());
+  const size_t i95 = std::min<size_t>(
+    fb.size() - 1, (size_t)std::ceil(0.95 * (double)fb.size()) - 1);
+  const double ms_per_thread = avg_cycles / hz * 1e3;
+  metrics[0] = ms_per_call;
+  metrics[1] = avg_calls;
+  metrics[2] = frac_thread;
+  metrics[3] = fb[i95];
+  metrics[4] = serialized;
+  metrics[5] = ms_per_thread > 0.0 && ms_opt > 0.0 ? ms_per_thread / ms_opt : 0.0;
+  metrics[6] = avg_cycles;
+  metrics[7] = ms_per_thread;
   return ZEUS_OK;
 }
 

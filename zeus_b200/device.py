@@ -84,7 +84,7 @@ class BfgsRun:
     """Preallocated outputs + workspace for repeated BFGS launches."""
 
     def __init__(self, obj, n: int, cfg: BfgsConfig, device="cuda",
-                 traj: bool = False, counters: bool = True):
+                 traj: bool = False, counters: bool = True, cycles: bool = False):
         self.dp = _as_problem(obj, device)
         self.n, self.cfg = n, cfg
         dim = self.dp.obj.dim
@@ -96,6 +96,9 @@ class BfgsRun:
         self.gnorm = torch.empty((n,), **f64)
         self.x = torch.empty((n, dim), **f64)
         self.counters = torch.zeros((n, 3), dtype=torch.int64, device=device) if counters else None
+        # per run {gradient, update, whole-run} clock64 cycles (sampled only
+        # when asked for)
+        self.cycles = torch.zeros((n, 3), dtype=torch.int64, device=device) if cycles else None
         self.control = torch.zeros((2,), **i32)
         self.traj = None
         if traj:
@@ -112,7 +115,7 @@ class BfgsRun:
         self.out = RunOutputs(_ptr(self.fval), _ptr(self.status), _ptr(self.iter),
                               _ptr(self.gnorm), _ptr(self.x), _ptr(self.counters),
                               _ptr(t.get("x")), _ptr(t.get("f")), _ptr(t.get("g")),
-                              _ptr(t.get("status")))
+                              _ptr(t.get("status")), _ptr(self.cycles))
 
     def launch(self, starts: torch.Tensor, stream=None, reset_control=True):
         if starts.dtype != torch.float64 or not starts.is_cuda or not starts.is_contiguous():
@@ -132,13 +135,14 @@ def bfgs_device(obj, starts: torch.Tensor, max_iter: int = 10000,
                 required: Optional[int] = None, tol: float = 1e-8,
                 mode: str = "fast", gradient: str = "adjoint",
                 layout: int = LAYOUT_AUTO, tile: int = 0, block: int = 0,
-                traj: bool = False, stream=None, flags: int = 0) -> BfgsRun:
+                traj: bool = False, stream=None, flags: int = 0,
+                cycles: bool = False) -> BfgsRun:
     """One BFGS per row of ``starts``; returns the BfgsRun with its outputs."""
     n = starts.shape[0]
     if required is None:
         required = n + 1  # stop-early off
     cfg = make_config(max_iter, required, tol, mode, gradient, layout, tile, block, flags)
-    r = BfgsRun(obj, n, cfg, device=starts.device, traj=traj)
+    r = BfgsRun(obj, n, cfg, device=starts.device, traj=traj, cycles=cycles)
     return r.launch(starts, stream=stream)
 
 
@@ -197,7 +201,7 @@ class BatchJob:
 
     def __init__(self, obj, starts: torch.Tensor, required: Optional[int] = None,
                  layout: int = LAYOUT_AUTO, tile: int = 0, runs_per_instance: int = 0,
-                 counters: bool = True):
+                 counters: bool = True, cycles: bool = False):
         self.dp = obj if isinstance(obj, DeviceProblem) else DeviceProblem(obj, starts.device)
         if starts.dtype != torch.float64 or not starts.is_cuda or not starts.is_contiguous():
             raise ValueError("starts must be a contiguous float64 CUDA tensor")
@@ -214,12 +218,14 @@ class BatchJob:
         self.x = torch.empty((self.n, dim), dtype=torch.float64, device=dev)
         self.counters = (torch.zeros((self.n, 3), dtype=torch.int64, device=dev)
                          if counters else None)
+        self.cycles = (torch.zeros((self.n, 3), dtype=torch.int64, device=dev)
+                       if cycles else None)
         self.control = torch.zeros((2,), dtype=torch.int32, device=dev)
 
     def c(self) -> BatchClass:
         out = RunOutputs(_ptr(self.fval), _ptr(self.status), _ptr(self.iter),
                          _ptr(self.gnorm), _ptr(self.x), _ptr(self.counters),
-                         None, None, None, None)
+                         None, None, None, None, _ptr(self.cycles))
         prob = self.dp.c()
         if self.rpi and self.dp.idata is not None:
             # ndata is per instance
@@ -287,3 +293,34 @@ def nll_sensitivity(job: "BatchJob", stream=None):
                                             _ptr(job.fval), _ptr(job.x), _ptr(best),
                                             _ptr(sens), _stream_handle(stream)))
     return best, sens
+
+
+METRIC_NAMES = ("ms_per_call", "calls_per_thread_mean", "fraction_of_thread", "block95",
+                "serialized", "fraction_of_kernel", "avg_cycles_per_thread",
+                "avg_ms_per_thread")
+
+
+def cycle_metrics(cycles, counters, ms_opt: float, sm_clock_khz: float,
+                  runs_per_block: int = 128) -> dict:
+    """The reference's AD and BFGS timer summaries
+    (bfgs_sequential.cuh:236-373) from per-run cycles and counters ((n, 3)
+    int64 arrays or tensors, host or device) of one launch of ms_opt ms:
+    {"ad": {...}, "bfgs": {...}} with METRIC_NAMES keys (the first five in
+    the order the results file writes them)."""
+    cyc = np.ascontiguousarray(_host_i64(cycles))
+    cnt = np.ascontiguousarray(_host_i64(counters))
+    if cyc.shape != cnt.shape or cyc.ndim != 2 or cyc.shape[1] != 3:
+        raise ValueError("cycles and counters must both be (n, 3)")
+    out = {}
+    for which, name in ((0, "ad"), (1, "bfgs")):
+        m = (C.c_double * 8)()
+        check(lib().zeus_cycle_metrics(cyc.ctypes.data, cnt.ctypes.data, cyc.shape[0], which,
+                                       float(sm_clock_khz), float(ms_opt), runs_per_block, m))
+        out[name] = dict(zip(METRIC_NAMES, list(m)))
+    return out
+
+
+def _host_i64(a):
+    if isinstance(a, torch.Tensor):
+        a = a.detach().cpu().numpy()
+    return np.asarray(a, dtype=np.int64)
