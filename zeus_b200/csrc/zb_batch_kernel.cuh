@@ -75,18 +75,33 @@ namespace zb {
       }
     }
 
-    // The per-run bodies (row, CTA, tile, thread) are called, not inlined:
-    // each is then compiled as a function of its own, with its own register
-    // assignment and scheduling, instead of sharing them with every other
-    // layout's body in the one kernel (measured: a 64-D row-layout run 1.94
-    // us an iteration inlined beside the tile, thread and CTA bodies, 1.49 us
-    // alone).
+    // The CTA, tile and thread bodies are called, not inlined, in a batch
+    // with row or CTA classes: each is then compiled as a function of its
+    // own, with its own register assignment and scheduling, instead of
+    // sharing them with every other layout's body in the one kernel
+    // (measured: a 64-D row-layout run 1.94 us an iteration inlined beside
+    // the tile, thread and CTA bodies, 1.49 us alone).  The row bodies stay
+    // inline in that kernel (the mixed batch 20.71 -> 20.37 ms, the 128-D
+    // iteration 3.18 -> 3.10 us); the kernel for batches without row or CTA
+    // classes never runs them and keeps them out of line (inlined there
+    // they cost the multimodal batch 8%).
     template <class F, int D, int NW>
     __device__ __noinline__ void
-    batch_row_run(const F f, double* gsm, int bar, int base, const BfgsParams prm,
-                  const double* x0, int64_t run, const RunOut out, Control* ctl)
+    batch_row_call(const F f, double* gsm, int bar, int base, const BfgsParams prm,
+                   const double* x0, int64_t run, const RunOut out, Control* ctl)
     {
       row_run<F, D, NW, true>(f, gsm, bar, base, prm, x0, run, out, ctl);
+    }
+
+    template <bool kInline, class F, int D, int NW>
+    __device__ __forceinline__ void
+    batch_row_run(const F& f, double* gsm, int bar, int base, const BfgsParams& prm,
+                  const double* x0, int64_t run, const RunOut& out, Control* ctl)
+    {
+      if constexpr (kInline)
+        batch_row_call<F, D, NW>(f, gsm, bar, base, prm, x0, run, out, ctl);
+      else
+        row_run<F, D, NW, true>(f, gsm, bar, base, prm, x0, run, out, ctl);
     }
 
     template <class F, int D, int kBlock>
@@ -214,7 +229,7 @@ namespace zb {
                 asm volatile("bar.sync %0, %1;" ::"r"(1 + gi), "n"(NT) : "memory");
                 if (r >= c.n)
                   break;
-                batch_row_run<F, D, NW>(instance_for(f, c, r), gsm, 1 + gi, gi * NT,
+                batch_row_run<kInline, F, D, NW>(instance_for(f, c, r), gsm, 1 + gi, gi * NT,
                                         prm, c.starts + r * D, r, c.out, c.ctl);
               }
             }
