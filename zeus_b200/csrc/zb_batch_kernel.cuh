@@ -85,23 +85,23 @@ namespace zb {
     // iteration 3.18 -> 3.10 us); the kernel for batches without row or CTA
     // classes never runs them and keeps them out of line (inlined there
     // they cost the multimodal batch 8%).
-    template <class F, int D, int NW>
+    template <class F, int D, int NW, int KS>
     __device__ __noinline__ void
     batch_row_call(const F f, double* gsm, int bar, int base, const BfgsParams prm,
                    const double* x0, int64_t run, const RunOut out, Control* ctl)
     {
-      row_run<F, D, NW, true>(f, gsm, bar, base, prm, x0, run, out, ctl);
+      row_run<F, D, NW, true, false, KS>(f, gsm, bar, base, prm, x0, run, out, ctl);
     }
 
-    template <bool kInline, class F, int D, int NW>
+    template <bool kInline, class F, int D, int NW, int KS>
     __device__ __forceinline__ void
     batch_row_run(const F& f, double* gsm, int bar, int base, const BfgsParams& prm,
                   const double* x0, int64_t run, const RunOut& out, Control* ctl)
     {
       if constexpr (kInline)
-        batch_row_call<F, D, NW>(f, gsm, bar, base, prm, x0, run, out, ctl);
+        batch_row_call<F, D, NW, KS>(f, gsm, bar, base, prm, x0, run, out, ctl);
       else
-        row_run<F, D, NW, true>(f, gsm, bar, base, prm, x0, run, out, ctl);
+        row_run<F, D, NW, true, false, KS>(f, gsm, bar, base, prm, x0, run, out, ctl);
     }
 
     template <class F, int D, int kBlock>
@@ -204,10 +204,15 @@ namespace zb {
     const bool early = (int)blockIdx.x < bt.early_b;
     for (int pass = 0; pass < 2; ++pass) {
       if ((pass == 0) != early) {
-        // phase A, row-layout classes: the block splits into groups of S*D
-        // threads, each taking runs from the class queue on its own
+        // phase A, row-layout classes: the block splits into groups of NW
+        // warps, each taking runs from the class queue on its own.  (Split
+        // groups, two 128-D runs a block with part of H in shared memory,
+        // measured slower here than in their own kernel -- 19.9 against 15.8
+        // ms for the 128-D class: the body spills under the batch kernel's
+        // register budget, and with 222 KB of shared memory in use the spills
+        // miss L1.  The batch keeps one 12-warp group for D = 128.)
         for (int ci = 0; ci < ncls; ++ci) {
-          const BatchClass c = classes[ci];
+          const BatchClass& c = classes[ci];
           if (c.layout != ZEUS_LAYOUT_ROWS)
             continue;
           const BfgsParams prm{c.n, bt.max_iter, c.required, bt.tol, bt.flags};
@@ -215,12 +220,20 @@ namespace zb {
             using F = decltype(f);
             constexpr int D = (int)F::arity;
             constexpr int NW = row_warps(D, kBlock);
+            constexpr int KS = 0;
             if constexpr (NW > 0 && D >= kBatchRowMinDim && RowLayoutObjective<F>) {
               constexpr int NT = 32 * NW;
+              // the host sizes shared memory for this shape: a launch given
+              // less (a host/device mismatch) runs none of the class's runs
+              // rather than reach past the end of shared memory
+              unsigned dyn;
+              asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+              if ((size_t)(kBlock / NT) * row_smem_doubles<D, NW, KS>() * sizeof(double) > dyn)
+                return;
               const int gi = (int)threadIdx.x / NT;
-              double* gsm = sm + (size_t)gi * row_smem_doubles<D, NW>();
+              double* gsm = sm + (size_t)gi * row_smem_doubles<D, NW, KS>();
               long long* slot =
-                reinterpret_cast<long long*>(gsm + row_smem_doubles<D, NW>() - 2);
+                reinterpret_cast<long long*>(gsm + row_smem_doubles<D, NW, KS>() - 2);
               for (;;) {
                 if ((int)threadIdx.x % NT == 0)
                   *slot = (long long)atomicAdd(c.queue, 1ull);
@@ -229,8 +242,9 @@ namespace zb {
                 asm volatile("bar.sync %0, %1;" ::"r"(1 + gi), "n"(NT) : "memory");
                 if (r >= c.n)
                   break;
-                batch_row_run<kInline, F, D, NW>(instance_for(f, c, r), gsm, 1 + gi, gi * NT,
-                                        prm, c.starts + r * D, r, c.out, c.ctl);
+                batch_row_run<kInline, F, D, NW, KS>(instance_for(f, c, r), gsm, 1 + gi,
+                                                     gi * NT, prm, c.starts + r * D, r,
+                                                     c.out, c.ctl);
               }
             }
           });
@@ -238,7 +252,7 @@ namespace zb {
         }
         // phase A, CTA-layout classes, one run per block at a time
         for (int ci = 0; ci < ncls; ++ci) {
-          const BatchClass c = classes[ci];
+          const BatchClass& c = classes[ci];
           if (c.layout != ZEUS_LAYOUT_CTA)
             continue;
           const BfgsParams prm{c.n, bt.max_iter, c.required, bt.tol, bt.flags};
@@ -274,7 +288,7 @@ namespace zb {
                      : batch_tile_buf_doubles(classes[ci].dim, classes[ci].tile);
       double* warp_buf = sm + (size_t)(threadIdx.x >> 5) * stride;
       for (int ci = 0; ci < ncls; ++ci) {
-        const BatchClass c = classes[ci];
+        const BatchClass& c = classes[ci];
         if (c.layout == ZEUS_LAYOUT_CTA || c.layout == ZEUS_LAYOUT_ROWS)
           continue;
         const BfgsParams prm{c.n, bt.max_iter, c.required, bt.tol, bt.flags};

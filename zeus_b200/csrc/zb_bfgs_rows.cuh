@@ -68,16 +68,17 @@ namespace zb {
   }
 
   // Shared memory of one group (doubles): x | p | g[2] | {s, w, y, g_x}[D]
-  // | row partial sums 2 x NW x D | trial points NG at the padded stride |
-  // trial values 32 | reductions | scratch NT | run slot 2.  Every part is
-  // an even number of doubles, so the parts stay 16-byte aligned.
+  // | row partial sums 2 x NW x D | trial points 21 at the padded stride |
+  // trial values 32 | reductions | scratch NT | the last KS columns of every
+  // thread's H segment, KS x R x NT | run slot 2.  Every part is an even
+  // number of doubles, so the parts stay 16-byte aligned.
   __host__ __device__ constexpr int
-  row_smem_doubles_rt(int d, int nw)
+  row_smem_doubles_rt(int d, int nw, int ks = 0)
   {
     const int nt = 32 * nw, de = (d + 1) & ~1, st = row_trial_width(nw);
-    const int ng = nw * (32 / st);
-    return 4 * de + 4 * d + 2 * nw * de + ng * ((row_trial_stride(d, st) + 1) & ~1) + 32 +
-           row_red_doubles(nw) + nt + 2;
+    const int ntx = kLineSearchTrials + 1; // trial points stored: the 21 trials
+    return 4 * de + 4 * d + 2 * nw * de + ntx * ((row_trial_stride(d, st) + 1) & ~1) + 32 +
+           row_red_doubles(nw) + nt + ks * (d / 32) * nt + 2;
   }
 
   template <int D, int NWG>
@@ -96,11 +97,11 @@ namespace zb {
                   "one round of trial groups, judged by one ballot");
   };
 
-  template <int D, int NW>
+  template <int D, int NW, int KS = 0>
   __host__ __device__ constexpr int
   row_smem_doubles()
   {
-    return row_smem_doubles_rt(D, NW);
+    return row_smem_doubles_rt(D, NW, KS);
   }
 
   template <class F>
@@ -154,10 +155,13 @@ namespace zb {
     !Adjoint || HasGradientCoop<F, G> || HasAdjointCoop<F, G>;
 
   // One run on the group, trial points stored: `sm` holds
-  // row_smem_doubles<D, NW>() doubles (16-byte aligned); the group is
+  // row_smem_doubles<D, NW, KS>() doubles (16-byte aligned); the group is
   // threads [base, base + 32 NW) of the block, synchronised by named
-  // barrier `bar`.
-  template <class F, int D, int NW, bool Adjoint, bool kTimed = false>
+  // barrier `bar`.  With KS > 0 the last KS columns of each thread's H
+  // segment live in shared memory (thread-major: a warp's accesses are
+  // consecutive), the rest in registers, so that a group of half the warps
+  // holds the same H and two groups share a block.
+  template <class F, int D, int NW, bool Adjoint, bool kTimed = false, int KS = 0>
   __device__ __forceinline__ void
   row_run_points(const F& f, double* sm, int bar, int base, const BfgsParams& prm,
                  const double* __restrict__ x0, int64_t run, const RunOut& out,
@@ -166,6 +170,9 @@ namespace zb {
     using RS = RowShape<D, NW>;
     constexpr int NT = RS::NT, R = RS::R, CW = RS::CW, ST = RS::ST, TPW = RS::TPW;
     constexpr int DE = RS::DE, TSTR = RS::TSTR;
+    constexpr int KR = CW - KS; // columns in registers
+    static_assert(KS >= 0 && KR >= 1 && (KS == 0 || R % 2 == 0),
+                  "shared columns hold row pairs");
     double* X = sm;
     double* P = X + DE;
     double* G = P + DE; // two slots of DE
@@ -177,7 +184,7 @@ namespace zb {
     double* YG = SW + 2 * D;
     double* PART = SW + 4 * D;
     double* TX = PART + 2 * NW * DE;
-    double* TF = TX + RS::NG * TSTR;
+    double* TF = TX + (kLineSearchTrials + 1) * TSTR;
     double* red = TF + 32;
     double* scratch = red + row_red_doubles(NW);
     const RowGroup<NT> grp{base, bar, red, scratch};
@@ -185,13 +192,22 @@ namespace zb {
     const int j0 = lw * CW, r0 = lane * R; // my columns and rows
     const bool owner = t < D;              // thread oi(r) keeps coordinate r
     const int r = owner ? (t % 32) * R + t / 32 : 0;
+    // rows q, q + 1 of shared column KR + c: HS[(c * R / 2 + q / 2) * NT + t]
+    double2* HS = reinterpret_cast<double2*>(scratch + NT);
 
-    double H[R][CW];
+    double H[R][KR];
 #pragma unroll
     for (int q = 0; q < R; ++q)
 #pragma unroll
-      for (int k = 0; k < CW; ++k)
+      for (int k = 0; k < KR; ++k)
         H[q][k] = (j0 + k == r0 + q) ? 1.0 : 0.0;
+#pragma unroll
+    for (int c = 0; c < KS; ++c)
+#pragma unroll
+      for (int q = 0; q < R; q += 2)
+        HS[(c * R / 2 + q / 2) * NT + t] =
+          make_double2(j0 + KR + c == r0 + q ? 1.0 : 0.0,
+                       j0 + KR + c == r0 + q + 1 ? 1.0 : 0.0);
     for (int i = t; i < D; i += NT)
       X[i] = x0[i];
     grp.sync();
@@ -329,11 +345,27 @@ namespace zb {
             const int oj = (j % R) * 32 + j / R;
             const double2 sw = *reinterpret_cast<const double2*>(SW + 2 * oj);
             const double2 yg = *reinterpret_cast<const double2*>(YG + 2 * oj);
+            if (k < KR) {
 #pragma unroll
-            for (int q = 0; q < R; ++q) {
-              H[q][k] = fma(sr[q], sw.y, fma(wr[q], sw.x, H[q][k]));
-              au[q] = fma(H[q][k], yg.x, au[q]);
-              ah[q] = fma(H[q][k], yg.y, ah[q]);
+              for (int q = 0; q < R; ++q) {
+                H[q][k < KR ? k : 0] =
+                  fma(sr[q], sw.y, fma(wr[q], sw.x, H[q][k < KR ? k : 0]));
+                au[q] = fma(H[q][k < KR ? k : 0], yg.x, au[q]);
+                ah[q] = fma(H[q][k < KR ? k : 0], yg.y, ah[q]);
+              }
+            } else {
+#pragma unroll
+              for (int q = 0; q < R; q += 2) {
+                double2* hp = HS + ((k - KR) * R / 2 + q / 2) * NT + t;
+                double2 h = *hp;
+                h.x = fma(sr[q], sw.y, fma(wr[q], sw.x, h.x));
+                h.y = fma(sr[q + 1], sw.y, fma(wr[q + 1], sw.x, h.y));
+                *hp = h;
+                au[q] = fma(h.x, yg.x, au[q]);
+                ah[q] = fma(h.x, yg.y, ah[q]);
+                au[q + 1] = fma(h.y, yg.x, au[q + 1]);
+                ah[q + 1] = fma(h.y, yg.y, ah[q + 1]);
+              }
             }
           }
         }
@@ -344,10 +376,21 @@ namespace zb {
           if (D % NW == 0 || j < D) {
             const int oj = (j % R) * 32 + j / R;
             const double2 yg = *reinterpret_cast<const double2*>(YG + 2 * oj);
+            if (k < KR) {
 #pragma unroll
-            for (int q = 0; q < R; ++q) {
-              au[q] = fma(H[q][k], yg.x, au[q]);
-              ah[q] = fma(H[q][k], yg.y, ah[q]);
+              for (int q = 0; q < R; ++q) {
+                au[q] = fma(H[q][k < KR ? k : 0], yg.x, au[q]);
+                ah[q] = fma(H[q][k < KR ? k : 0], yg.y, ah[q]);
+              }
+            } else {
+#pragma unroll
+              for (int q = 0; q < R; q += 2) {
+                const double2 h = HS[((k - KR) * R / 2 + q / 2) * NT + t];
+                au[q] = fma(h.x, yg.x, au[q]);
+                ah[q] = fma(h.x, yg.y, ah[q]);
+                au[q + 1] = fma(h.y, yg.x, au[q + 1]);
+                ah[q + 1] = fma(h.y, yg.y, ah[q + 1]);
+              }
             }
           }
         }
@@ -804,17 +847,17 @@ namespace zb {
   // more than the two barriers saved.)
   inline constexpr int kRowLineMaxDim = 64;
 
-  template <class F, int D, int NW, bool Adjoint, bool kTimed = false>
+  template <class F, int D, int NW, bool Adjoint, bool kTimed = false, int KS = 0>
   __device__ __forceinline__ void
   row_run(const F& f, double* sm, int bar, int base, const BfgsParams& prm,
           const double* __restrict__ x0, int64_t run, const RunOut& out,
           Control* ctl)
   {
-    if constexpr (Adjoint && RowLineObjective<F> && D <= kRowLineMaxDim)
+    if constexpr (KS == 0 && Adjoint && RowLineObjective<F> && D <= kRowLineMaxDim)
       row_run_line<F, D, NW, kTimed>(f, sm, bar, base, prm, x0, run, out, ctl);
     else
-      row_run_points<F, D, NW, Adjoint, kTimed>(f, sm, bar, base, prm, x0, run, out,
-                                                ctl);
+      row_run_points<F, D, NW, Adjoint, kTimed, KS>(f, sm, bar, base, prm, x0, run,
+                                                    out, ctl);
   }
 
   // Warps of a group for D in a block of `block` threads: among the counts
@@ -847,19 +890,59 @@ namespace zb {
     return 0;
   }
 
-  // Standalone launches: one group per block, blocks take runs from the
-  // workspace queue as they finish (block b starts with run b).
-  template <class F, int D, int NW, bool Adjoint, bool kTimed = false>
-  __global__ void __launch_bounds__(32 * NW)
+  // H doubles a thread of a split group keeps in registers: those of a
+  // thread of the unsplit group (44 at D = 128), which the batch kernel's
+  // register budget holds without spilling in the sweep.
+  inline constexpr int kRowSplitRegDoubles = 44;
+
+  // Split groups (the standalone row kernel): where one group of
+  // row_warps(d, block) warps fills the whole block (D = 128 at 384
+  // threads: twelve warps), two blocks of half the warps share the SM
+  // instead, each thread keeping as many columns of its segment in registers
+  // as before and the last `row_split_cols` in shared memory.  Two runs then
+  // go through an SM at once, one's barriers and reductions overlapping the
+  // other's sweep: the 128-D class of 1365 runs 14.1 -> 11.1 ms on a B200,
+  // though one run alone is slower (3.18 against 2.80 us an iteration).
+  __host__ __device__ constexpr int
+  row_split_warps(int d, int block)
+  {
+    const int nw = row_warps(d, block);
+    return (nw > 0 && 32 * nw == block && block <= 384 && d >= 128 && nw % 2 == 0)
+             ? nw / 2
+             : 0;
+  }
+  __host__ __device__ constexpr int
+  row_split_cols(int d, int block)
+  {
+    const int nw2 = row_split_warps(d, block);
+    if (!nw2)
+      return 0;
+    const int r = d / 32, cw = (d + nw2 - 1) / nw2, kr = kRowSplitRegDoubles / r;
+    return cw > kr ? cw - kr : 0;
+  }
+  // Warps of one group and shared columns per thread in a block of `block`
+  __host__ __device__ constexpr int
+  row_group_warps(int d, int block)
+  {
+    return row_split_warps(d, block) ? row_split_warps(d, block) : row_warps(d, block);
+  }
+
+  // Standalone launches: one group per block (two blocks per SM for split
+  // groups, the registers of the two summing to one full block's), blocks
+  // take runs from the workspace queue as they finish (block b starts with
+  // run b).
+  template <class F, int D, int NW, bool Adjoint, bool kTimed = false, int KS = 0>
+  __global__ void __launch_bounds__(32 * NW, KS > 0 ? 2 : 1)
     bfgs_rows_kernel(F f, BfgsParams prm, const double* __restrict__ starts,
                      RunOut out, Control* ctl, unsigned long long* queue)
   {
     extern __shared__ __align__(16) double sm[];
     constexpr int NT = 32 * NW;
-    double* slot = sm + row_smem_doubles<D, NW>() - 2;
+    double* slot = sm + row_smem_doubles<D, NW, KS>() - 2;
     int64_t run = blockIdx.x;
     while (run < prm.n) {
-      row_run<F, D, NW, Adjoint, kTimed>(f, sm, 1, 0, prm, starts + run * D, run, out, ctl);
+      row_run<F, D, NW, Adjoint, kTimed, KS>(f, sm, 1, 0, prm, starts + run * D, run, out,
+                                             ctl);
       if (threadIdx.x == 0)
         reinterpret_cast<long long*>(slot)[0] =
           (long long)gridDim.x + (long long)atomicAdd(queue, 1ull);

@@ -82,9 +82,11 @@ namespace zb {
                     const RunOut& out, Control* ctl, void* ws, size_t ws_bytes,
                     cudaStream_t st)
     {
-      constexpr int NW = row_warps(D, kRowBlockCap), NT = 32 * NW;
-      const size_t smem = sizeof(double) * row_smem_doubles<D, NW>();
-      auto kern = bfgs_rows_kernel<F, D, NW, Adj, kTimed>;
+      // the batch's groups: split groups for D = 128, two blocks per SM
+      constexpr int NW = row_group_warps(D, kRowBlockCap), NT = 32 * NW;
+      constexpr int KS = row_split_cols(D, kRowBlockCap);
+      const size_t smem = sizeof(double) * row_smem_doubles<D, NW, KS>();
+      auto kern = bfgs_rows_kernel<F, D, NW, Adj, kTimed, KS>;
       int rc = cuda_fail(cudaFuncSetAttribute(
                            kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem),
