@@ -111,8 +111,8 @@ def algorithmic_flops(jobs_counters) -> float:
 #  * gaussian150: the CTA-layout BFGS kernel at full size (1.50 MB read: C,
 #    the starts and the first touch of the outputs).
 MEASURED_TRAFFIC = {
-    "mixed": (8 * 551168, "1/8-size capture x 8"),
-    "gaussian150": (1502208, "full-size capture"),
+    "mixed": (8 * (582912 + 9216), "1/8-size capture x 8"),
+    "gaussian150": (1503232, "full-size capture"),
 }
 
 

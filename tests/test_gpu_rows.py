@@ -1,8 +1,10 @@
-"""The row layout (zb_bfgs_rows.cuh): one run per group of S*D threads, each
-thread holding a segment of one row of H in registers, several groups per
-block.  Checked against the oracle on final results (fast-mode arithmetic),
-and the persistent batch's row groups against standalone row launches bit
-for bit (same per-run body, same segment count)."""
+"""The row layout (zb_bfgs_rows.cuh): one run per group of warps, each
+thread holding a segment of R rows of H in registers (split groups: part
+of it in shared memory), several groups per block.  Checked against the
+oracle on final results (fast-mode arithmetic), and the persistent batch's
+row classes against standalone row launches bit for bit (same per-run
+body, same group shape; a 128-D class at 384 threads runs the standalone
+kernel itself beside the batch kernel)."""
 import numpy as np
 import pytest
 import torch
@@ -44,7 +46,7 @@ def test_rows_against_oracle(cuda, dim, n, iters, grad):
                                                abs=1e-14)
 
 
-@pytest.mark.parametrize("block,dims", [(384, (32, 64)), (512, (64,))])
+@pytest.mark.parametrize("block,dims", [(384, (32, 64, 128)), (512, (64,))])
 def test_batch_rows_equal_standalone(cuda, block, dims):
     jobs, sts = [], []
     for i, d in enumerate(dims):
@@ -67,10 +69,9 @@ def test_batch_rows_equal_standalone(cuda, block, dims):
 
 @pytest.mark.parametrize("block", [384, 512])
 def test_batch_rows_dim128_against_oracle(cuda, block):
-    """The batch's 128-D groups (twelve warps at 384 threads, sixteen at 512)
-    differ from the standalone kernel's split groups (six warps, two blocks
-    an SM, part of H in shared memory) in summation order only: each is
-    checked against the oracle."""
+    """A 128-D class runs in the standalone kernel's split groups beside the
+    batch kernel at 384 threads (a companion launch) and in sixteen-warp
+    groups inside the 512-thread batch kernel: both against the oracle."""
     st = O.oracle_starts(77, 32, 128, -5.0, 5.0)
     want = O.oracle_bfgs(0, 128, st, max_iter=1500)
     j = BatchJob(zb.Rosenbrock(128), torch.from_numpy(st).cuda(), layout=zb.LAYOUT_ROWS)

@@ -2,6 +2,7 @@
 // classes, picks layouts and the block size, and launches one of the kernel
 // instantiations (zb_batch_512.cu, zb_batch_384.cu).
 #include <algorithm>
+#include <map>
 #include <vector>
 
 #include "zb_batch.cuh"
@@ -93,13 +94,66 @@ namespace zb {
                : 1;
     }
 
+    // Companion classes: row-layout classes whose standalone kernel runs two
+    // split groups an SM (D = 128: six warps each, part of H in shared
+    // memory).  Inside the batch kernel those groups spill under its
+    // register budget, and one 12-warp group runs the class at 3.3 us an
+    // iteration per SM against 2.35 in the standalone kernel; so such a
+    // class runs in its standalone kernel, launched right after the batch
+    // kernel on a second stream: its blocks take each SM as the batch's
+    // block there retires (most within a few ms; those holding runs that
+    // iterate to MAX_ITER stay), and both end about together.
+    constexpr int kCompanionQueueBytes = 256;
+
+    bool
+    companion_class(const zeus_problem& p, int layout, int block)
+    {
+      return layout == ZEUS_LAYOUT_ROWS && block == kBatchBlockSmall &&
+             row_split_warps(p.dim, kBatchBlockSmall) > 0 &&
+             rows_layout_supported(p.kind, p.dim);
+    }
+
+    // A second stream and a fork / join event pair per device and host
+    // thread, made once (never destroyed: exit-safe).
+    struct SideStream {
+      cudaStream_t st = nullptr;
+      cudaEvent_t fork = nullptr, join = nullptr;
+    };
+
+    int
+    side_stream(SideStream** out)
+    {
+      thread_local std::map<int, SideStream> per_dev;
+      int dev = 0;
+      int rc = cuda_fail(cudaGetDevice(&dev), "current device");
+      if (rc)
+        return rc;
+      SideStream& s = per_dev[dev];
+      if (!s.st) {
+        if ((rc = cuda_fail(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking),
+                            "batch side stream")) ||
+            (rc = cuda_fail(cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming),
+                            "batch fork event")) ||
+            (rc = cuda_fail(cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming),
+                            "batch join event"))) {
+          s = SideStream{};
+          return rc;
+        }
+      }
+      *out = &s;
+      return ZEUS_OK;
+    }
+
     size_t
     ws_layout(const zeus_batch_class* cls, int ncls, size_t* off_queue,
               std::vector<size_t>* off_bins)
     {
       size_t b = 0;
       *off_queue = b;
+      // the batch's per-class queues, then a standalone run queue per class
+      // (used by companion classes)
       b += align_up(sizeof(unsigned long long) * (size_t)ncls);
+      b += align_up((size_t)kCompanionQueueBytes * ncls);
       off_bins->assign(ncls, 0);
       for (int i = 0; i < ncls; ++i)
         if (cls[i].problem.kind == ZEUS_OBJ_POISSON_NLL) {
@@ -156,7 +210,10 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
   cudaStream_t st = (cudaStream_t)stream;
   char* ws = static_cast<char*>(d_workspace);
   auto* queues = reinterpret_cast<unsigned long long*>(ws + off_q);
+  char* companion_ws =
+    ws + off_q + align_up(sizeof(unsigned long long) * (size_t)n_classes);
   std::vector<BatchClass> hc;
+  std::vector<int> hc_index; // each entry's position in `classes`
   hc.reserve(n_classes);
   size_t smem_tile = 0;
   double warp_runs = 0.0;
@@ -219,6 +276,7 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
     else if (layout == ZEUS_LAYOUT_THREAD)
       warp_runs += (double)c.n / 32.0;
     hc.push_back(b);
+    hc_index.push_back(i);
   }
   // Block size: 512 threads (16 warps per SM) for a throughput batch -- only
   // tile/thread classes, all of dimension 8 or less, more than two waves of
@@ -239,6 +297,21 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
     if (b.layout == ZEUS_LAYOUT_CTA &&
         cta_doubles_rt(b.kind, b.dim, block) * sizeof(double) > 227 * 1024)
       block = kBatchBlockSmall; // its CTA classes fit at 384 (checked above)
+  // companion classes leave the batch table for their standalone kernel
+  std::vector<BatchClass> companions;
+  std::vector<int> companion_index;
+  {
+    std::vector<BatchClass> keep;
+    for (size_t k = 0; k < hc.size(); ++k) {
+      if (companion_class(classes[hc_index[k]].problem, hc[k].layout, block)) {
+        companions.push_back(hc[k]);
+        companion_index.push_back(hc_index[k]);
+      } else {
+        keep.push_back(hc[k]);
+      }
+    }
+    hc.swap(keep);
+  }
   size_t smem_cta = 0;
   for (const BatchClass& b : hc) {
     if (b.layout == ZEUS_LAYOUT_CTA)
@@ -265,7 +338,7 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
   if (rc)
     return rc;
   BatchTable bt{};
-  bt.ncls = n_classes;
+  bt.ncls = (int)hc.size();
   bt.max_iter = config->max_iter;
   bt.tol = config->tolerance;
   bt.flags = config->flags;
@@ -280,12 +353,46 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
   }
   constexpr int kEarlyDiv = 16;
   bt.early_b = has_cta && has_warp ? std::max(1, sm_count() / kEarlyDiv) : 0;
-  for (int i = 0; i < n_classes; ++i)
+  for (int i = 0; i < bt.ncls; ++i)
     bt.c[i] = hc[i];
   const size_t smem =
     sizeof(double) * std::max(smem_cta, smem_tile * (block / 32));
-  return block == kBatchBlockLarge ? launch_batch_512(bt, smem, st)
-                                   : launch_batch_384(bt, smem, st);
+  const auto launch_batch = [&]() -> int {
+    if (bt.ncls == 0)
+      return ZEUS_OK;
+    return block == kBatchBlockLarge ? launch_batch_512(bt, smem, st)
+                                     : launch_batch_384(bt, smem, st);
+  };
+  if (companions.empty())
+    return launch_batch();
+  // the batch kernel first (its blocks take the SMs), then the companions
+  // on the side stream, joined back into `st`
+  SideStream* side = nullptr;
+  if ((rc = side_stream(&side)) ||
+      (rc = cuda_fail(cudaEventRecord(side->fork, st), "batch fork")) ||
+      (rc = launch_batch()) ||
+      (rc = cuda_fail(cudaStreamWaitEvent(side->st, side->fork, 0), "batch fork wait")))
+    return rc;
+  zeus_bfgs_config rows_cfg = *config;
+  rows_cfg.layout = ZEUS_LAYOUT_ROWS;
+  rows_cfg.tile = 0;
+  for (size_t k = 0; k < companions.size(); ++k) {
+    const BatchClass& b = companions[k];
+    if (b.n <= 0)
+      continue;
+    const zeus_problem& p = classes[companion_index[k]].problem;
+    const Objective o{p.kind, p.dim, p.data, p.idata, p.ndata, p.flags, nullptr};
+    const BfgsParams prm{b.n, config->max_iter, b.required, config->tolerance,
+                         config->flags};
+    if ((rc = launch_rows(o, rows_cfg, prm, b.starts, b.out, b.ctl,
+                          companion_ws + (size_t)companion_index[k] * kCompanionQueueBytes,
+                          kCompanionQueueBytes, side->st)))
+      break;
+  }
+  // join even after a failed launch, so that `st` is left consistent
+  const int jrc = cuda_fail(cudaEventRecord(side->join, side->st), "batch join");
+  const int wrc = cuda_fail(cudaStreamWaitEvent(st, side->join, 0), "batch join wait");
+  return rc ? rc : jrc ? jrc : wrc;
 }
 
 } // extern "C"
