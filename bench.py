@@ -111,7 +111,7 @@ def algorithmic_flops(jobs_counters) -> float:
 #  * gaussian150: the CTA-layout BFGS kernel at full size (1.50 MB read: C,
 #    the starts and the first touch of the outputs).
 MEASURED_TRAFFIC = {
-    "mixed": (8 * (582912 + 9216), "1/8-size capture x 8"),
+    "mixed": (8 * (600064 + 1024), "1/8-size capture x 8, batch kernel"),
     "gaussian150": (1503232, "full-size capture"),
 }
 
@@ -414,6 +414,10 @@ def run_gpu(args, rank, world, local_rank):
             tuned[j.name] = {"layout": ["auto", "thread", "tile", "cta", "rows"][lay], "tile": tile,
                              "sample_ms": ms}
     batch = Batch([s["bj"] for s in state], jobs[0].max_iter, jobs[0].tol) if wl["batch"] else None
+    # row classes of D >= 128 run beside the batch kernel as a companion
+    # launch of the standalone row kernel (zeus_batch_device)
+    companions = sum(1 for s in state if tuned.get(s["job"].name, {}).get("layout") == "rows"
+                     and s["obj"].dim >= 128) if batch is not None else 0
 
     def gen_starts(s):
         j, prob = s["job"], s["dp"].c()
@@ -442,7 +446,7 @@ def run_gpu(args, rank, world, local_rank):
         e0.record(stream)
         if batch is not None:
             batch.launch(stream)
-            launches += 1 + sum(1 for s in state if s["nbins"])
+            launches += 1 + companions + sum(1 for s in state if s["nbins"])
             outs = [s["bj"] for s in state]
         else:
             for s in state:
@@ -647,8 +651,10 @@ def run_gpu(args, rank, world, local_rank):
                      "autotuned_layouts": tuned},
             "converged_per_step": conv_all,
             "plain_dual": plain,
-            "roofline": {"bound": "fp64", "kernel": "bfgs_batch_kernel" if batch is not None
-                         else "bfgs (standalone launches)",
+            "roofline": {"bound": "fp64",
+                         "kernel": ("bfgs_batch_kernel" + (" + bfgs_rows_kernel (companion)"
+                                                           if companions else ""))
+                         if batch is not None else "bfgs (standalone launches)",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": (achieved / peak) if peak else None,
                          "peak_source": "measured FP64 FMA probe on this GPU "
