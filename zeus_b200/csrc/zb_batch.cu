@@ -323,13 +323,18 @@ zeus_batch_device(const zeus_batch_class* classes, int32_t n_classes,
   // batch lasts as long as its slowest run, and a class whose bulk finishes
   // early lets its stalled runs (those iterating to MAX_ITER) overlap the
   // bigger classes' bulk instead of starting after it (the mixed batch:
-  // 44.0 ms largest-first, 40.0 ms smallest-first).  Then the tile/thread
-  // classes, largest dimension first.
+  // 44.0 ms largest-first, 40.0 ms smallest-first).  Row classes (all
+  // light beside a companion 128-D class) largest dimension first: their
+  // longest MAX_ITER runs, the 64-D ones (14.5 ms), then start at once (the
+  // mixed batch 17.9 -> 17.2 / 18.1 ms in two runs: within its run-to-run
+  // spread).  Then the tile/thread classes, largest dimension first.
   std::stable_sort(hc.begin(), hc.end(), [](const BatchClass& a, const BatchClass& b) {
     const int ka = a.layout == ZEUS_LAYOUT_CTA || a.layout == ZEUS_LAYOUT_ROWS;
     const int kb = b.layout == ZEUS_LAYOUT_CTA || b.layout == ZEUS_LAYOUT_ROWS;
     if (ka != kb)
       return ka > kb;
+    if (a.layout == ZEUS_LAYOUT_ROWS && b.layout == ZEUS_LAYOUT_ROWS)
+      return a.dim > b.dim;
     return ka ? a.dim < b.dim : a.dim > b.dim;
   });
   int rc = cuda_fail(cudaMemsetAsync(queues, 0,
