@@ -94,7 +94,10 @@ def nll_starts(n, seed=11):
 # Measured floor of runs whose 50 exact-mode iterates stay within 1e-10 of the
 # reference's: CUDA's cos/exp/log/pow/lgamma differ from glibc's by an ulp now
 # and then, and a line-search decision taken on f values that differ in the
-# last bit sends the two trajectories apart.
+# last bit sends the two trajectories apart.  Rounding alone does as much:
+# the oracle built with FMA contraction (same libm, only the rounding of
+# a*b+c differs) keeps 19% of these NLL runs and 56% of the Rastrigin-10
+# runs within 1e-10 of the plain oracle (tests/test_rounding_sensitivity.py).
 MIN_WITHIN = {RAS: 0.75, ACK: 0.75, NLL: 0.25}
 
 
