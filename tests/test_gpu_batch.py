@@ -141,3 +141,34 @@ def test_autotune_records_a_built_layout(cuda, obj, lo, hi):
     torch.cuda.synchronize()
     for k in auto:
         np.testing.assert_array_equal(auto[k], expl[k], err_msg=k)
+
+
+def test_batch_with_companion_in_a_cuda_graph(cuda):
+    """A batch whose 128-D row class runs as a companion launch (a second
+    stream forked from and joined back into the caller's) captured into a
+    CUDA graph and replayed gives the same runs as the direct launch."""
+    from zeus_b200.device import Batch, BatchJob, starts_uniform
+
+    jobs = [BatchJob(zb.Rosenbrock(128), starts_uniform(3, 40, 128, -5.0, 5.0),
+                     layout=zb.LAYOUT_ROWS),
+            BatchJob(zb.Rosenbrock(8), starts_uniform(4, 200, 8, -5.0, 5.0))]
+    b = Batch(jobs, max_iter=600)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        b.launch(s)  # direct: also makes the library's side stream
+    torch.cuda.synchronize()
+    want = [(j.fval.clone(), j.status.clone(), j.x.clone()) for j in jobs]
+    for j in jobs:
+        j.fval.fill_(float("nan"))
+        j.status.fill_(-7)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=s, capture_error_mode="thread_local"):
+        b.launch(s, reset=False)
+    for j in jobs:
+        j.control.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    for j, (f, st, x) in zip(jobs, want):
+        assert torch.equal(j.status, st)
+        assert torch.equal(j.fval, f)
+        assert torch.equal(j.x, x)
