@@ -1,6 +1,7 @@
 """ctypes access to the checkers: the C restatement (oracle/libzeus_oracle.so)
 and the reference's own sequential BFGS compiled for the host
-(oracle/_ref/libzeus_ref.so).  Test infrastructure only."""
+(oracle/_ref/libzeus_ref.so) and for the GPU (oracle/_ref/libzeus_ref_gpu.so).
+Test infrastructure only."""
 from __future__ import annotations
 
 import ctypes as C
@@ -12,6 +13,7 @@ ROOT = Path(__file__).resolve().parent.parent
 ORACLE_SO = ROOT / "oracle" / "libzeus_oracle.so"
 ORACLE_FMA_SO = ROOT / "oracle" / "libzeus_oracle_fma.so"
 REF_SO = ROOT / "oracle" / "_ref" / "libzeus_ref.so"
+REF_GPU_SO = ROOT / "oracle" / "_ref" / "libzeus_ref_gpu.so"
 
 _P = C.c_void_p
 _BFGS_SIG = [C.c_int, C.c_int, _P, _P, C.c_int, _P, C.c_int, C.c_double, C.c_double,
@@ -142,6 +144,24 @@ def oracle_bfgs(*a, **k):
 
 def ref_bfgs(*a, **k):
     return run_bfgs(ref().zref_bfgs, *a, **k)
+
+
+_ref_gpu = None
+
+
+def ref_gpu_available() -> bool:
+    return REF_GPU_SO.exists()
+
+
+def ref_gpu_bfgs(*a, **k):
+    """The reference's sequential BFGS kernel run on the GPU (cuda:0), same
+    arguments and results as ref_bfgs."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        L = C.CDLL(str(REF_GPU_SO))
+        L.zrefg_bfgs.argtypes = _BFGS_SIG
+        _ref_gpu = L
+    return run_bfgs(_ref_gpu.zrefg_bfgs, *a, **k)
 
 
 PRNG_XORWOW, PRNG_PHILOX, PRNG_SOBOL = 0, 1, 2

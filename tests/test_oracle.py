@@ -369,3 +369,13 @@ def test_reference_ackley_gradient_near_origin():
     for fn in (O.grad_dual, O.ref_grad_dual):
         _, g = fn(ACK, 2, np.array([-1e-17, 1e-17]))
         np.testing.assert_allclose(g, [-2.0, 2.0], rtol=1e-12)
+
+
+@pytest.mark.skipif(not O.ref_gpu_available(), reason="oracle/_ref GPU build not built")
+def test_reference_gpu_build_loads_without_a_gpu():
+    """The reference kernel's GPU build (the checker of exact mode on the
+    device) loads here and exports its entry point; it runs only under -m gpu."""
+    import ctypes
+
+    lib = ctypes.CDLL(str(O.REF_GPU_SO))
+    assert hasattr(lib, "zrefg_bfgs")
