@@ -10,13 +10,9 @@ are compiled without FMA contraction and keep the reference's operation order,
 and every iterate, f, gradient norm and status must agree bit for bit.
 
 The reference's host build differs from its GPU build only in the libm; the
-share of runs on which those two agree is printed beside the result.
-
-Opt-in: runs when ZEUS_CHECK_REFERENCE_KERNEL=1 is set (it launches the
-reference's own kernel, which takes its two D x D matrices from the device
-heap)."""
-import os
-
+share of runs on which those two agree is printed beside the result (on a
+B200: all runs for Rosenbrock, 0-6% for the cos/exp/log/pow/lgamma
+objectives -- the whole of the difference the CPU comparison sees)."""
 import numpy as np
 import pytest
 
@@ -24,11 +20,7 @@ from tests import _oracle as O
 from tests.test_gpu_parity import (ACK, BOUNDS, NLL, RAS, ROS, gpu_run, make_obj,
                                    nll_starts)
 
-pytestmark = [
-    pytest.mark.gpu,
-    pytest.mark.skipif(os.environ.get("ZEUS_CHECK_REFERENCE_KERNEL") != "1",
-                       reason="opt-in: set ZEUS_CHECK_REFERENCE_KERNEL=1"),
-]
+pytestmark = pytest.mark.gpu
 
 KEYS = ("status", "iter", "fval", "gnorm", "x", "traj_x", "traj_f", "traj_g",
         "traj_status")
