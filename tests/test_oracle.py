@@ -379,3 +379,23 @@ def test_reference_gpu_build_loads_without_a_gpu():
 
     lib = ctypes.CDLL(str(O.REF_GPU_SO))
     assert hasattr(lib, "zrefg_bfgs")
+
+
+@needs_ref
+@pytest.mark.parametrize("kind,dim,n,iters", [(ROS, 64, 2, 30), (ROS, 128, 1, 8),
+                                              (GAU, 150, 1, 5)])
+def test_oracle_bit_identical_at_the_benchmarked_dimensions(kind, dim, n, iters):
+    """The oracle's hoisted O(D^3) update against the reference's O(D^4) loop
+    (utils.cuh:245-287) at the sizes whose run-for-run fixtures the oracle
+    wrote (Rosenbrock 64 and 128 of the mixed batch, the 150-D Gaussian):
+    every iterate, f, gradient norm and status, bit for bit."""
+    data = None
+    if kind == GAU:
+        data = np.full((dim, dim), 0.5)  # C_ii = 75.5, C_ij = 0.5 at dim 150
+        np.fill_diagonal(data, 1.0 + (dim - 1) * 0.5)
+    st = O.oracle_starts(42, n, dim, -5.0, 5.0)
+    a = O.oracle_bfgs(kind, dim, st, max_iter=iters, data=data, traj=True)
+    b = O.ref_bfgs(kind, dim, st, max_iter=iters, data=data, traj=True)
+    for key in ("fval", "status", "iter", "gnorm", "x", "traj_x", "traj_f", "traj_g",
+                "traj_status"):
+        np.testing.assert_array_equal(a[key], b[key], err_msg=key)
